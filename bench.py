@@ -1,0 +1,335 @@
+"""Benchmark of the B200-native DTC-SpMM path.
+
+Workload (default): power-law graph SpMM -- R-MAT(0.57, 0.19, 0.19, 0.05),
+2^20 nodes, 16 * 2^20 generated edges, symmetrised + self-loops + duplicates
+removed, GCN-normalised values; B = 2^20 x 128 fp32 N(0,1); seeded synthetic
+data standing in for the reference's graph datasets.
+
+One step = one SpMM C = A * B over the whole matrix with A's ME-TCF arrays and
+B already resident in HBM (`value`, GFLOP/s = 2 * nnz * N / t). `e2e` runs the
+reference-facing call (DTCSpMM.run_DTCSpMM) with B in pinned host memory and
+copies C back to the host inside the timed region.
+
+  python bench.py [--gpus N --steps K --warmup W]     # our kernels
+  python bench.py --impl reference                    # host CSR SpMM (CPU arm)
+
+Multi-GPU (torchrun): every rank runs its own replica of the workload (row
+windows are independent; there is no data-path collective); timing is the
+max over ranks, `value` the sum of the ranks' work over that time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dtc-spmm_asplos24_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def make_workload(args):
+    from dtc_b200 import gen
+    if args.config == "rmat":
+        A = gen.rmat(args.scale, 16.0, 0.57, 0.19, 0.19, seed=0)
+        N = args.N or 128
+        name = f"rmat-2^{args.scale}-sym-gcn-N{N}"
+    elif args.config == "stencil":
+        A = gen.stencil27(126, seed=0)
+        N = args.N or 256
+        name = f"stencil27-126^3-N{N}"
+    else:
+        A = gen.uniform(4096, mean=8.0, seed=0)
+        N = args.N or 32
+        name = f"uniform-4096-poisson8-N{N}"
+    B = gen.normal(A.K, N, seed=1)
+    return A, B, N, name
+
+
+def algorithmic_bytes(m, N, b_elem_bytes, with_values=True):
+    """ME-TCF structure + gathered B rows (distinct per window) + C write."""
+    import torch
+    T, nnz = m.T, m.nnz
+    s2x = m.SparseAToX.view(T, m.W)
+    valid = (s2x != 0)
+    valid[:, 0] = True
+    U = int(valid.sum().item())
+    S = nnz * (1 + (4 if with_values else 0)) + 8 * T * 4 + (T + 1) * 4 + (m.nwin + 1) * 4
+    return S + U * N * b_elem_bytes + m.M * N * 4, U, S
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks / throttle reasons during the timed region."""
+
+    def __init__(self, idx):
+        self.idx = idx
+        self.p = None
+        self.path = os.path.join("/tmp", f"dtc_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines()]
+        except OSError:
+            return None
+        rows = [r for r in rows if len(r) >= 9]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9])
+                          if v.strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(A, B, N, gpu_C=None, budget_s=15.0):
+    """Host FP32 CSR SpMM (the oracle's OpenMP port) on all host cores.
+
+    Bounded sample: the full matrix, repeated while the budget lasts (at least
+    twice). Also checks the GPU result against the FP64 oracle on a row sample.
+    """
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    C = np.empty((A.M, N), np.float32)
+    O.spmm_f32(A.rowptr, A.col, A.val, A.M, B, nthreads=cores, out=C)  # warm-up
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < 2 or (time.perf_counter() < t_end and len(times) < 10):
+        t0 = time.perf_counter()
+        O.spmm_f32(A.rowptr, A.col, A.val, A.M, B, nthreads=cores, out=C)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    flops = 2.0 * A.nnz * N
+    out = {"value": flops / t / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+           "sample": f"full matrix ({A.nnz} nnz x N={N}), median of {len(times)} runs",
+           "cpu_model": _cpu_model()}
+    err = None
+    if gpu_C is not None:
+        err = accuracy_vs_fp64(A, B, N, gpu_C)
+    return out, err
+
+
+def accuracy_vs_fp64(A, B, N, gpu_C, rows_per=64):
+    """Relative Frobenius and max-abs error of the GPU result vs the FP64
+    oracle on every `rows_per`-th row window (16 rows each)."""
+    from oracle import oracle as O
+    wins = np.arange(0, (A.M + 15) // 16, rows_per)
+    rows = np.concatenate([np.arange(w * 16, min(w * 16 + 16, A.M)) for w in wins])
+    lens = A.rowptr[rows + 1] - A.rowptr[rows]
+    rp = np.zeros(len(rows) + 1, np.int64)
+    rp[1:] = np.cumsum(lens)
+    idx = np.concatenate([np.arange(A.rowptr[r], A.rowptr[r + 1]) for r in rows])
+    C64 = O.spmm_f64(rp.astype(np.int32), A.col[idx], A.val[idx], len(rows), B)
+    G = gpu_C[rows].astype(np.float64)
+    return {"rel_fro": float(np.linalg.norm(G - C64) / np.linalg.norm(C64)),
+            "max_abs": float(np.abs(G - C64).max()), "rows_checked": int(len(rows))}
+
+
+def _cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_reference_arm(args, rank, world):
+    """CPU arm: the reference has no CPU SpMM, so its arm is the oracle's host
+    CSR SpMM port on all host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    A, B, N, name = make_workload(args)
+    cores = os.cpu_count() or 1
+    from oracle import oracle as O
+    C = np.empty((A.M, N), np.float32)
+    for _ in range(max(1, min(args.warmup, 2))):
+        O.spmm_f32(A.rowptr, A.col, A.val, A.M, B, nthreads=cores, out=C)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.spmm_f32(A.rowptr, A.col, A.val, A.M, B, nthreads=cores, out=C)
+        ts.append(time.perf_counter() - t0)
+    t = float(np.mean(ts))
+    v = 2.0 * A.nnz * N / t / 1e9
+    line = {"impl": "reference", "metric": "SpMM GFLOP/s (2*nnz*N)", "value": v,
+            "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": name, "nnz": A.nnz, "num_nodes": A.M, "N": N},
+            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                             "sample": f"full matrix, {args.steps} steps"},
+            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="rmat", choices=["rmat", "stencil", "uniform"])
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--N", type=int, default=0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from dtc_b200 import metcf
+    import DTCSpMM
+
+    A, Bh, N, name = make_workload(args)
+    dev = torch.device("cuda", local)
+    m = metcf.convert(A.rowptr, A.col, A.M, values=A.val, device=dev)
+    B = torch.from_numpy(Bh).to(dev)
+    Cd = torch.empty((A.M, N), dtype=torch.float32, device=dev)
+    flops = 2.0 * A.nnz * N
+    peaks, peak_kind = load_peaks()
+
+    # forms measured (same matrix, same B)
+    forms = {
+        "tf32_window": lambda: metcf.spmm(m, B, out=Cd),
+        "tf32_balance": lambda: metcf.spmm_balance(m, B, out=Cd, workspace=ws_bal),
+    }
+    ws_bal = torch.empty(metcf.spmm_balance_workspace_bytes(m, N), dtype=torch.uint8, device=dev)
+    launches = {"tf32_window": 1, "tf32_balance": 3}
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for a, b in evs:
+            a.record()
+            fn()
+            b.record()
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        per = [a.elapsed_time(b) for a, b in evs]
+        total = float(e0.elapsed_time(e1))
+        if dist:
+            t = torch.tensor([total], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total / steps, per, wall
+
+    results = {}
+    for k, fn in forms.items():
+        ms, per, _ = timed(fn, max(3, args.steps // 2), args.warmup)
+        results[k] = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9}
+    best = min(results, key=lambda k: results[k]["ms"])
+
+    # headline timed region: K steps of the best form, clocks sampled
+    with Clocks(local) as clk:
+        ms, per, wall = timed(forms[best], args.steps, args.warmup)
+    clocks = clk.summary()
+    value = world * flops / (ms * 1e-3) / 1e9
+
+    nbytes, U, S = algorithmic_bytes(m, N, 4)
+    kern_ms = float(np.mean(per))
+    achieved = nbytes / (kern_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "peak_kind": peak_kind, "algorithmic_bytes": nbytes, "distinct_rows_U": U,
+                "metcf_bytes": S, "compulsory_bytes": S + A.K * N * 4 + A.M * N * 4,
+                "kernel": best, "kernel_ms": kern_ms}
+
+    # end-to-end through the reference-facing API: pinned host B -> device,
+    # run_DTCSpMM, C -> pinned host
+    Bpin = torch.from_numpy(Bh).pin_memory()
+    Cpin = torch.empty((A.M, N), dtype=torch.float32).pin_memory()
+    Bdev = torch.empty_like(B)
+
+    def e2e_step():
+        Bdev.copy_(Bpin, non_blocking=True)
+        C = DTCSpMM.run_DTCSpMM(Bdev, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                                m.SparseAToX, A.M, A.nnz, "float_nonsplit", values=m.TCvalues)[0]
+        Cpin.copy_(C, non_blocking=True)
+
+    e2e_steps = max(3, min(args.steps, 10))
+    e_ms, _, _ = timed(e2e_step, e2e_steps, 2)
+    e2e = {"value": world * flops / (e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+           "h2d_bytes_per_step": int(Bh.nbytes), "d2h_bytes_per_step": int(A.M * N * 4),
+           "api": "DTCSpMM.run_DTCSpMM"}
+
+    cpu, err = (None, None)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        forms[best]()
+        torch.cuda.synchronize()
+        cpu, err = cpu_baseline(A, Bh, N, gpu_C=Cd.cpu().numpy())
+
+    if rank == 0:
+        line = {"metric": "SpMM GFLOP/s (2*nnz*N) & HBM-roofline %", "value": value,
+                "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "tf32", "data": "synthetic",
+                "config": {"workload": name, "num_nodes": A.M, "nnz": A.nnz, "N": N,
+                           "T": m.T, "form": best, "l2": "inputs larger than L2 (B 512 MiB,"
+                           " ME-TCF %.0f MB); no flush" % (S / 1e6)},
+                "forms": results, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
+                "accuracy_vs_fp64": err, "clocks": clocks,
+                "gpu_launches": launches[best] * args.steps}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

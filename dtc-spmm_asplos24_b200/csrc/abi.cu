@@ -1,0 +1,224 @@
+// C-ABI entry points of libdtcspmm.so (declared in include/dtc_spmm.h):
+// argument checks, status/error text, per-device state, dispatch.
+#include <mutex>
+#include <string>
+#include "common.cuh"
+
+namespace dtc {
+
+dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                          const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                          int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
+                          float* part, cudaStream_t st);
+dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                           int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
+                           int precision, float* C, int mode, int grid, float* part,
+                           cudaStream_t st);
+size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
+dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
+                        cudaStream_t st);
+dtc_status spmm_mma_sync_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                              const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                              const float* B, int32_t N, float* C, cudaStream_t st);
+dtc_status pack_b_impl(int fmt, const float* B, int64_t rows, int32_t N, void* p0, void* p1,
+                       cudaStream_t st);
+dtc_status bformat_bytes_impl(int fmt, int64_t rows, int32_t N, size_t* b0, size_t* b1);
+
+namespace {
+thread_local std::string g_last_error;
+__device__ uint32_t g_device_error;
+constexpr int kMaxDev = 64;
+std::mutex g_mu;
+int g_sms[kMaxDev] = {};
+int g_major[kMaxDev] = {};
+uint32_t* g_err_ptr[kMaxDev] = {};
+
+int cur_dev() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d & (kMaxDev - 1);
+}
+
+void fill_dev_props(int d) {
+  if (g_sms[d]) return;
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+  g_sms[d] = v > 0 ? v : 1;
+  cudaDeviceGetAttribute(&v, cudaDevAttrComputeCapabilityMajor, d);
+  g_major[d] = v;
+}
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+dtc_status cuda_status(cudaError_t e, const char* what) {
+  g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return DTC_ERR_CUDA;
+}
+
+int num_sms() {
+  int d = cur_dev();
+  std::lock_guard<std::mutex> lk(g_mu);
+  fill_dev_props(d);
+  return g_sms[d];
+}
+
+bool is_sm100() {
+  int d = cur_dev();
+  std::lock_guard<std::mutex> lk(g_mu);
+  fill_dev_props(d);
+  return g_major[d] == 10;
+}
+
+uint32_t* device_error_word() {
+  int d = cur_dev();
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_err_ptr[d]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_device_error) == cudaSuccess) g_err_ptr[d] = (uint32_t*)p;
+  }
+  return g_err_ptr[d];
+}
+
+}  // namespace dtc
+
+using namespace dtc;
+
+extern "C" {
+
+const char* dtc_last_error(void) { return g_last_error.c_str(); }
+
+int dtc_version(void) { return 100; }
+
+/* Reads (and optionally clears) the device-side error word: bit 0 = a
+ * bounded wait gave up, bit 1 = an out-of-range index was skipped.
+ * Synchronises the device. */
+dtc_status dtc_device_status(uint32_t* flags, int clear) {
+  DTC_REQUIRE(flags != nullptr, "flags is null");
+  uint32_t* p = device_error_word();
+  if (!p) { set_error("device error word unavailable"); return DTC_ERR_CUDA; }
+  DTC_CUDA(cudaDeviceSynchronize());
+  DTC_CUDA(cudaMemcpy(flags, p, 4, cudaMemcpyDeviceToHost));
+  if (clear) DTC_CUDA(cudaMemset(p, 0, 4));
+  return DTC_OK;
+}
+
+dtc_status dtc_rowid_to_window_offset(const int32_t* d_tcblockRowid, int64_t num_blocks,
+                                      int32_t num_windows, int32_t* d_rowWindowOffset,
+                                      dtc_stream_t stream) {
+  DTC_REQUIRE(num_blocks >= 0 && num_windows >= 0, "bad sizes");
+  DTC_REQUIRE(d_rowWindowOffset != nullptr, "null rowWindowOffset");
+  DTC_REQUIRE(num_blocks == 0 || d_tcblockRowid != nullptr, "null tcblockRowid");
+  return rowid_to_rwo(d_tcblockRowid, num_blocks, num_windows, d_rowWindowOffset,
+                      (cudaStream_t)stream);
+}
+
+dtc_status dtc_spmm(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                    const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                    const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                    int64_t num_blocks, const float* d_B, int32_t N, float* d_C,
+                    dtc_stream_t stream) {
+  DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_B && d_C, "null device pointer");
+  DTC_REQUIRE(num_blocks == 0 || (d_tileId && d_sparseAToX), "null device pointer");
+  if (N % 4 != 0)
+    return spmm_mma_sync_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
+                              d_tcValues, num_nodes, num_windows, d_B, N, d_C,
+                              (cudaStream_t)stream);
+  return spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
+                        num_nodes, num_windows, num_blocks, d_B, N, d_C, 0, 0, nullptr,
+                        (cudaStream_t)stream);
+}
+
+dtc_status dtc_spmm_balance_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                            size_t* bytes) {
+  DTC_REQUIRE(bytes != nullptr, "bytes is null");
+  DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
+  int32_t nwin = (num_nodes + 15) / 16;
+  *bytes = align_up((size_t)(nwin + 1) * 4, 256) + spmm_partials_bytes(num_blocks, N, 0);
+  return DTC_OK;
+}
+
+dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tileId,
+                            const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                            const float* d_tcValues, int32_t num_nodes, int64_t num_blocks,
+                            const float* d_B, int32_t N, float* d_C, void* d_workspace,
+                            size_t workspace_bytes, dtc_stream_t stream) {
+  size_t need = 0;
+  dtc_status s = dtc_spmm_balance_workspace_bytes(num_nodes, num_blocks, N, &need);
+  if (s != DTC_OK) return s;
+  DTC_REQUIRE(d_tcblockOffset && d_B && d_C, "null device pointer");
+  DTC_REQUIRE(num_blocks == 0 || (d_tcblockRowid && d_tileId && d_sparseAToX),
+              "null device pointer");
+  if (!d_workspace || workspace_bytes < need) {
+    set_error("balance workspace too small");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  int32_t nwin = (num_nodes + 15) / 16;
+  int32_t* rwo = (int32_t*)d_workspace;
+  float* part = (float*)((char*)d_workspace + align_up((size_t)(nwin + 1) * 4, 256));
+  s = rowid_to_rwo(d_tcblockRowid, num_blocks, nwin, rwo, st);
+  if (s != DTC_OK) return s;
+  if (N % 4 != 0)
+    return spmm_mma_sync_impl(rwo, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
+                              num_nodes, nwin, d_B, N, d_C, st);
+  return spmm_tf32_impl(rwo, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues, num_nodes,
+                        nwin, num_blocks, d_B, N, d_C, 1, 0, part, st);
+}
+
+dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
+                                       int grid, size_t* bytes) {
+  DTC_REQUIRE(bytes != nullptr, "bytes is null");
+  DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
+  *bytes = (mode == 1) ? spmm_partials_bytes(num_blocks, N, grid) : 0;
+  return DTC_OK;
+}
+
+dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                       const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                       const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                       int64_t num_blocks, int bformat, const void* d_Bplane0,
+                       const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
+                       int grid, void* d_workspace, size_t workspace_bytes,
+                       dtc_stream_t stream) {
+  DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
+  DTC_REQUIRE(grid >= 0, "grid must be >= 0");
+  DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_Bplane0 && d_C, "null device pointer");
+  size_t need = 0;
+  dtc_status s = dtc_spmm_ex_workspace_bytes(num_nodes, num_blocks, N, mode, grid, &need);
+  if (s != DTC_OK) return s;
+  if (need > 0 && (!d_workspace || workspace_bytes < need)) {
+    set_error("spmm workspace too small");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
+    return spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
+                          d_tcValues, num_nodes, num_windows, num_blocks,
+                          (const float*)d_Bplane0, N, d_C, mode, grid, (float*)d_workspace, st);
+  return spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
+                         num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
+                         precision, d_C, mode, grid, (float*)d_workspace, st);
+}
+
+dtc_status dtc_spmm_mma_sync(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                             const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                             const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                             const float* d_B, int32_t N, float* d_C, dtc_stream_t stream) {
+  DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_B && d_C, "null device pointer");
+  return spmm_mma_sync_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
+                            d_tcValues, num_nodes, num_windows, d_B, N, d_C,
+                            (cudaStream_t)stream);
+}
+
+dtc_status dtc_bformat_bytes(int fmt, int64_t rows, int32_t N, size_t* plane0, size_t* plane1) {
+  return bformat_bytes_impl(fmt, rows, N, plane0, plane1);
+}
+
+dtc_status dtc_pack_b(int fmt, const float* d_B, int64_t rows, int32_t N, void* d_plane0,
+                      void* d_plane1, dtc_stream_t stream) {
+  return pack_b_impl(fmt, d_B, rows, N, d_plane0, d_plane1, (cudaStream_t)stream);
+}
+
+}  // extern "C"

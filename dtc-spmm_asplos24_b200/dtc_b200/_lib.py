@@ -1,0 +1,101 @@
+"""ctypes binding of the C ABI (include/dtc_spmm.h, lib/libdtcspmm.so).
+
+Every exported symbol is declared here with its argument types; ``call``
+raises ``DtcError`` with the library's error text on a non-zero status. No
+computation happens in Python: when the library is missing the import fails
+loudly (there is no fallback path).
+"""
+import ctypes as C
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(PKG_DIR, "lib")
+LIBDTC_PATH = os.path.join(LIB_DIR, "libdtcspmm.so")
+LIBGEN_PATH = os.path.join(LIB_DIR, "libdtcgen.so")
+
+i32, i64, u64, f64 = C.c_int32, C.c_int64, C.c_uint64, C.c_double
+vp, sz = C.c_void_p, C.c_size_t
+szp = C.POINTER(C.c_size_t)
+i64p = C.POINTER(C.c_int64)
+u32p = C.POINTER(C.c_uint32)
+
+# name -> argtypes (restype is dtc_status == int unless listed in _RESTYPES)
+SIGNATURES = {
+    "dtc_last_error": [],
+    "dtc_version": [],
+    "dtc_device_status": [u32p, C.c_int],
+    "dtc_convert_workspace_bytes": [i32, i64, i32, i32, szp],
+    "dtc_convert_count": [vp, vp, i32, i64, i32, i32, vp, vp, vp, vp, vp, sz, i64p, vp],
+    "dtc_convert_fill": [vp, vp, i32, i64, i32, i32, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp,
+                         vp, sz, vp],
+    "dtc_bformat_bytes": [C.c_int, i64, i32, szp, szp],
+    "dtc_pack_b": [C.c_int, vp, i64, i32, vp, vp, vp],
+    "dtc_spmm": [vp, vp, vp, vp, vp, i32, i32, i64, vp, i32, vp, vp],
+    "dtc_spmm_balance_workspace_bytes": [i32, i64, i32, szp],
+    "dtc_spmm_balance": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp, sz, vp],
+    "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
+                    C.c_int, C.c_int, vp, sz, vp],
+    "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, C.c_int, C.c_int, szp],
+    "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
+    "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
+}
+_RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int}
+
+B_F32, B_SPLIT24, B_BF16, B_FP8 = 0, 1, 2, 3
+PREC_TF32, PREC_SPLIT3, PREC_SPLIT4 = 0, 1, 2
+
+
+class DtcError(RuntimeError):
+    pass
+
+
+_lib = None
+_gen = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBDTC_PATH):
+            raise ImportError(f"{LIBDTC_PATH} is not built; run dtc-spmm_asplos24_b200/build.py")
+        L = C.CDLL(LIBDTC_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, C.c_int)
+        _lib = L
+    return _lib
+
+
+def call(name, *args):
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        msg = lib().dtc_last_error().decode(errors="replace")
+        raise DtcError(f"{name} -> status {rc}: {msg}")
+    return rc
+
+
+def gen():
+    global _gen
+    if _gen is None:
+        if not os.path.exists(LIBGEN_PATH):
+            raise ImportError(f"{LIBGEN_PATH} is not built; run dtc-spmm_asplos24_b200/build.py")
+        G = C.CDLL(LIBGEN_PATH)
+        G.dtcgen_uniform.argtypes = [i32, i32, f64, u64]
+        G.dtcgen_rmat.argtypes = [i32, f64, f64, f64, f64, u64]
+        G.dtcgen_stencil27.argtypes = [i32, u64]
+        G.dtcgen_zipf.argtypes = [i32, f64, i32, i32, u64]
+        G.dtcgen_banded.argtypes = [i32, i32, f64, u64]
+        G.dtcgen_blockdiag.argtypes = [i32, i32, i32, f64, u64]
+        for n in ("uniform", "rmat", "stencil27", "zipf", "banded", "blockdiag"):
+            getattr(G, "dtcgen_" + n).restype = vp
+        G.dtcgen_shape.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]
+        G.dtcgen_shape.restype = None
+        G.dtcgen_copy.argtypes = [vp, vp, vp, vp]
+        G.dtcgen_copy.restype = None
+        G.dtcgen_free.argtypes = [vp]
+        G.dtcgen_free.restype = None
+        G.dtcgen_normal.argtypes = [vp, i64, u64]
+        G.dtcgen_normal.restype = None
+        _gen = G
+    return _gen

@@ -1,0 +1,166 @@
+/*
+ * dtc_spmm.h -- C ABI of the B200-native DTC-SpMM path (libdtcspmm.so).
+ *
+ * Plain pointers and sizes only; every pointer named d_* is device memory on
+ * the current device, every call is asynchronous on `stream` unless stated,
+ * and every call returns a dtc_status (never exits the process). The library
+ * allocates no device memory: callers pass a workspace sized by the matching
+ * *_workspace_bytes query.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the reference project root, HPMLL/DTC-SpMM_ASPLOS24).
+ */
+#ifndef DTC_SPMM_H_
+#define DTC_SPMM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* dtc_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+  DTC_OK = 0,
+  DTC_ERR_INVALID_ARGUMENT = 1,   /* bad size, null pointer, unsupported shape */
+  DTC_ERR_WORKSPACE_TOO_SMALL = 2,
+  DTC_ERR_CUDA = 3,               /* a CUDA runtime call failed; see dtc_last_error() */
+  DTC_ERR_UNSUPPORTED = 4,        /* device or format not supported (e.g. not sm_100) */
+  DTC_ERR_DEVICE_CHECK = 5        /* a kernel's own bounds / wait check fired */
+} dtc_status;
+
+/* Human-readable text of the last error recorded on the calling host thread. */
+const char* dtc_last_error(void);
+
+/* Library version (major*10000 + minor*100 + patch). */
+int dtc_version(void);
+
+/* Reads the device-side error word of the current device into *flags and
+ * clears it if `clear` != 0 (synchronises the device). Bit 0: a bounded
+ * in-kernel wait gave up; bit 1: an out-of-range index was skipped. No
+ * reference counterpart (the reference has no device-side checks). */
+dtc_status dtc_device_status(uint32_t* flags, int clear);
+
+/* ------------------------------------------------------------------------- */
+/* ME-TCF conversion.                                                         */
+/* Replaces DTCSpMM.preprocess_gpu (DTC-SpMM/DTCSpMM.cpp:313-359) and its     */
+/* launchers fill_edgeToRow_cuda / fill_segment_cuda / seg_sort_dequ          */
+/* (DTC-SpMM/DTCSpMM_kernel.cu:107-419). Split in two phases because the      */
+/* output sizes depend on the block count T (the reference reads T back to    */
+/* the host at DTCSpMM_kernel.cu:378-380, so does dtc_convert_count).         */
+/* ------------------------------------------------------------------------- */
+
+/* Workspace for both conversion phases. */
+dtc_status dtc_convert_workspace_bytes(int32_t num_nodes, int64_t nnz, int32_t block_h,
+                                       int32_t block_w, size_t* bytes);
+
+/* Phase 1. Inputs: CSR d_col[nnz] (edgeList), d_rowptr[num_nodes+1] (nodePointer).
+ * Writes d_blockPartition[num_windows], d_edgeToColumn[nnz], d_edgeToRow[nnz]
+ * (the reference's in-place outputs) and d_rowWindowOffset[num_windows+1];
+ * stores T in *num_blocks (synchronises `stream`). block_h*block_w <= 256. */
+dtc_status dtc_convert_count(const int32_t* d_col, const int32_t* d_rowptr, int32_t num_nodes,
+                             int64_t nnz, int32_t block_h, int32_t block_w,
+                             int32_t* d_blockPartition, int32_t* d_edgeToColumn,
+                             int32_t* d_edgeToRow, int32_t* d_rowWindowOffset,
+                             void* d_workspace, size_t workspace_bytes, int64_t* num_blocks,
+                             dtc_stream_t stream);
+
+/* Phase 2. Writes d_tcblockRowid[T], d_tileId[nnz] (u8), d_tcblockOffset[T+1],
+ * d_sparseAToX[T*block_w]. If d_values (CSR order) is non-null, also writes
+ * d_tcValues[nnz] in tile order (duplicate (row,col) pairs of a block merged
+ * into their first occurrence, later ones 0) -- an array the reference lacks. */
+dtc_status dtc_convert_fill(const int32_t* d_col, const int32_t* d_rowptr, int32_t num_nodes,
+                            int64_t nnz, int32_t block_h, int32_t block_w,
+                            const int32_t* d_edgeToColumn, const int32_t* d_edgeToRow,
+                            const int32_t* d_rowWindowOffset, int64_t num_blocks,
+                            int32_t* d_tcblockRowid, uint8_t* d_tileId, int32_t* d_tcblockOffset,
+                            int32_t* d_sparseAToX, const float* d_values, float* d_tcValues,
+                            void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Dense-operand storage forms ("B formats").                                  */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+  DTC_B_F32 = 0,      /* fp32 rows; the TF32 drop-in form                      */
+  DTC_B_SPLIT24 = 1,  /* bf16 hi plane [rows*N] + u8 extension plane [rows*N]: */
+                      /* fp32 rounded to 16 significant bits, 3 bytes/element  */
+  DTC_B_BF16 = 2,     /* bf16 rows                                              */
+  DTC_B_FP8 = 3       /* e4m3 plane [rows*N] + fp32 per-row scale [rows]        */
+} dtc_bformat;
+
+typedef enum {
+  DTC_PREC_TF32 = 0,  /* tcgen05 kind::tf32, fp32 B                              */
+  DTC_PREC_SPLIT3 = 1,/* kind::f16 bf16: A_hi*B_hi + A_hi*B_lo + A_lo*B_hi       */
+  DTC_PREC_SPLIT4 = 2 /* kind::f16 bf16: (A_hi + A_lo) * (B_hi + B_lo), 4 terms  */
+} dtc_precision;
+
+/* Bytes of the two planes of `fmt` for a rows x N fp32 matrix. */
+dtc_status dtc_bformat_bytes(int fmt, int64_t rows, int32_t N, size_t* plane0, size_t* plane1);
+
+/* Converts fp32 d_B[rows*N] into `fmt` (plane1 unused for F32/BF16). */
+dtc_status dtc_pack_b(int fmt, const float* d_B, int64_t rows, int32_t N, void* d_plane0,
+                      void* d_plane1, dtc_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* TC-block SpMM  C[num_nodes x N] = A * B.                                    */
+/* ------------------------------------------------------------------------- */
+
+/* Window-scheduled SpMM. Replaces run_DTCSpMM / spmm_forward_ptx_uint8_improved
+ * (DTC-SpMM/DTCSpMM.cpp:117-131 -> DTCSpMM_kernel.cu:811-944) and DTCSpMM_gcn
+ * (DTCSpMM.cpp:147-161 -> DTCSpMM_kernel.cu:1033-1116): one launch, each row
+ * window is owned by one CTA, no workspace. d_tcValues == NULL reproduces the
+ * reference's implicit A = 1 (DTCSpMM_kernel.cu:837-838). C rows of empty
+ * windows are written as zeros (the reference zero-fills, :823). */
+dtc_status dtc_spmm(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                    const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                    const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                    int64_t num_blocks, const float* d_B, int32_t N, float* d_C,
+                    dtc_stream_t stream);
+
+/* Strict-balance SpMM. Replaces run_DTCSpMM_balance /
+ * spmm_balance_forward_ptx_uint8_prefetch (DTC-SpMM/DTCSpMM.cpp:163-178 ->
+ * DTCSpMM_kernel.cu:1118-1199, kernels :4730-4901, :5085-5362). Every CTA gets
+ * an equal contiguous range of TC blocks (windows split across CTAs); partial
+ * tiles go to the workspace and are reduced in fixed CTA order by a second
+ * kernel, so results are bitwise reproducible (the reference uses fp32
+ * atomicAdd). Needs only d_tcblockRowid, like the reference. */
+dtc_status dtc_spmm_balance_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                            size_t* bytes);
+dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tileId,
+                            const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                            const float* d_tcValues, int32_t num_nodes, int64_t num_blocks,
+                            const float* d_B, int32_t N, float* d_C, void* d_workspace,
+                            size_t workspace_bytes, dtc_stream_t stream);
+
+/* General form used by the tuned paths: any B format / precision, explicit
+ * schedule. mode 0 = window-scheduled, 1 = strict balance. grid = CTAs (0 =
+ * one per SM). d_rowWindowOffset is required (build it from TCblockRowid with
+ * dtc_rowid_to_window_offset). Workspace needed only for mode 1. */
+dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                       const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                       const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                       int64_t num_blocks, int bformat, const void* d_Bplane0,
+                       const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
+                       int grid, void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
+                                       int grid, size_t* bytes);
+
+/* d_rowWindowOffset[num_windows+1] from a sorted d_tcblockRowid[T]. */
+dtc_status dtc_rowid_to_window_offset(const int32_t* d_tcblockRowid, int64_t num_blocks,
+                                      int32_t num_windows, int32_t* d_rowWindowOffset,
+                                      dtc_stream_t stream);
+
+/* Legacy-ISA comparison kernel: the same product with sm_80-style
+ * mma.sync.m16n8k8 TF32, one warp group per row window (the instruction
+ * family of DTCSpMM_kernel.cu:2663-2866). Any N >= 1. */
+dtc_status dtc_spmm_mma_sync(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                             const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                             const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                             const float* d_B, int32_t N, float* d_C, dtc_stream_t stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+#endif  /* DTC_SPMM_H_ */

@@ -1,0 +1,130 @@
+"""ORACLE -- test infrastructure only (the checker, never the product path).
+
+numpy/ctypes front end of ``oracle/metcf_oracle.c``: the CPU restatement of the
+reference's ME-TCF conversion (DTC-SpMM/DTCSpMM_kernel.cu:107-419,
+DTC-SpMM/DTCSpMM.cpp:313-359) and FP64/FP32 CSR SpMM. Only tests/,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build_oracle  # noqa: F401  (package-relative when imported as oracle.oracle)
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build_oracle.build()
+        _lib = ctypes.CDLL(path)
+        i32p = ctypes.POINTER(ctypes.c_int32)
+        _lib.oracle_metcf_num_blocks.restype = ctypes.c_int64
+        _lib.oracle_metcf.restype = ctypes.c_int
+        _lib.oracle_metcf_values.restype = ctypes.c_int
+        del i32p
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _csr(rowptr, col):
+    return (np.ascontiguousarray(rowptr, dtype=np.int32),
+            np.ascontiguousarray(col, dtype=np.int32))
+
+
+def metcf(rowptr, col, M, H=16, W=8, values=None):
+    """Reference-exact ME-TCF arrays for a CSR matrix (dict of numpy arrays).
+
+    Keys follow the reference tuple (DTCSpMM.cpp:356-358) plus the in-place
+    outputs: RowWindowOffset, TCblockRowid, TCblocktileId, TCblockoffset,
+    SparseAToX, T, blockPartition, edgeToColumn, edgeToRow, and TCvalues when
+    ``values`` is given.
+    """
+    L = lib()
+    rowptr, col = _csr(rowptr, col)
+    nnz = int(rowptr[M])
+    nwin = (M + H - 1) // H
+    T = int(L.oracle_metcf_num_blocks(_p(rowptr), _p(col), ctypes.c_int32(M),
+                                      ctypes.c_int32(H), ctypes.c_int32(W)))
+    out = dict(
+        blockPartition=np.zeros(nwin, np.int32),
+        edgeToColumn=np.zeros(nnz, np.int32),
+        edgeToRow=np.zeros(nnz, np.int32),
+        RowWindowOffset=np.zeros(nwin + 1, np.int32),
+        TCblockRowid=np.zeros(T, np.int32),
+        TCblocktileId=np.zeros(nnz, np.uint8),
+        TCblockoffset=np.zeros(T + 1, np.int32),
+        SparseAToX=np.zeros(T * W, np.int32),
+    )
+    rc = L.oracle_metcf(_p(rowptr), _p(col), ctypes.c_int32(M), ctypes.c_int32(H),
+                        ctypes.c_int32(W), _p(out["blockPartition"]), _p(out["edgeToColumn"]),
+                        _p(out["edgeToRow"]), _p(out["RowWindowOffset"]),
+                        _p(out["TCblockRowid"]), _p(out["TCblocktileId"]),
+                        _p(out["TCblockoffset"]), _p(out["SparseAToX"]), ctypes.c_int64(T))
+    if rc != 0:
+        raise RuntimeError(f"oracle_metcf failed ({rc})")
+    out["T"] = T
+    if values is not None:
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        tv = np.zeros(nnz, np.float32)
+        L.oracle_metcf_values(_p(rowptr), _p(col), _p(v), ctypes.c_int32(M), ctypes.c_int32(H),
+                              ctypes.c_int32(W), _p(out["edgeToColumn"]), _p(out["edgeToRow"]),
+                              _p(out["RowWindowOffset"]), _p(out["TCblockoffset"]), _p(tv))
+        out["TCvalues"] = tv
+    return out
+
+
+def spmm_f64(rowptr, col, values, M, B):
+    """FP64 CSR SpMM; ``values=None`` = the reference's implicit A = 1."""
+    rowptr, col = _csr(rowptr, col)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    N = B.shape[1]
+    C = np.empty((M, N), np.float64)
+    v = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
+    lib().oracle_spmm_f64(_p(rowptr), _p(col), None if v is None else _p(v),
+                          ctypes.c_int32(M), ctypes.c_int32(N), _p(B), _p(C))
+    return C
+
+
+def spmm_absbound_f64(rowptr, col, values, M, B):
+    """sum_e |A[i,e]| |B[col_e, j]| per output element (tolerance scale)."""
+    rowptr, col = _csr(rowptr, col)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    N = B.shape[1]
+    C = np.empty((M, N), np.float64)
+    v = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
+    lib().oracle_spmm_absbound_f64(_p(rowptr), _p(col), None if v is None else _p(v),
+                                   ctypes.c_int32(M), ctypes.c_int32(N), _p(B), _p(C))
+    return C
+
+
+def spmm_f32(rowptr, col, values, M, B, nthreads=0, out=None):
+    """Host FP32 CSR SpMM over ``nthreads`` OpenMP threads (the CPU baseline)."""
+    rowptr, col = _csr(rowptr, col)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    N = B.shape[1]
+    C = out if out is not None else np.empty((M, N), np.float32)
+    v = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
+    lib().oracle_spmm_f32(_p(rowptr), _p(col), None if v is None else _p(v),
+                          ctypes.c_int32(M), ctypes.c_int32(N), _p(B), _p(C),
+                          ctypes.c_int(nthreads))
+    return C
+
+
+def metcf_spmm_f64(m, M, B, H=16, W=8, tc_values=None):
+    """FP64 product straight from ME-TCF arrays (tile semantics of the reference)."""
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    N = B.shape[1]
+    C = np.empty((M, N), np.float64)
+    tv = None if tc_values is None else np.ascontiguousarray(tc_values, dtype=np.float32)
+    lib().oracle_metcf_spmm_f64(_p(m["RowWindowOffset"]), _p(m["TCblocktileId"]),
+                                _p(m["TCblockoffset"]), _p(m["SparseAToX"]),
+                                None if tv is None else _p(tv), ctypes.c_int32(M),
+                                ctypes.c_int32(H), ctypes.c_int32(W), ctypes.c_int32(N),
+                                _p(B), _p(C))
+    return C

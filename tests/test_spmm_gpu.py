@@ -1,0 +1,170 @@
+"""GPU parity of the TC-block SpMM kernels (through the C ABI) against the
+FP64 oracle, the reference's own SpMM golden outputs and the all-ones KAT.
+
+Tolerance (TF32 form): |C - C64| <= 2^-9 * sum_e |a_e| |b_e| + 1e-6 per
+element: A is rounded to TF32 (2^-11), B is read by the tensor core at TF32
+precision (truncation, 2^-10), products accumulate in fp32.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.golden import cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TF32_TOL = 2.0 ** -9
+
+
+def _setup(name, N, seed=11):
+    import torch
+    from dtc_b200 import metcf
+    rp, col, val, M = cases.CASES[name]()
+    m = metcf.convert(rp, col, M, values=val)
+    B = np.random.default_rng(seed).standard_normal((M, N)).astype(np.float32)
+    return rp, col, val, M, m, B, torch.from_numpy(B).cuda()
+
+
+def _check(C, rp, col, val, M, B, tol=TF32_TOL):
+    C = C.cpu().numpy().astype(np.float64)
+    ref = O.spmm_f64(rp, col, val, M, B)
+    bound = O.spmm_absbound_f64(rp, col, val, M, B)
+    err = np.abs(C - ref)
+    lim = tol * bound + 1e-6
+    bad = err > lim
+    assert not bad.any(), (f"{bad.sum()} elements out of tolerance; worst "
+                           f"{(err - lim).max():.3e} at {np.unravel_index(np.argmax(err - lim), err.shape)}")
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+@pytest.mark.parametrize("N", [16, 64, 128])
+def test_window_spmm_vs_fp64(cuda, name, N):
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup(name, N)
+    _check(metcf.spmm(m, Bt), rp, col, val, M, B)
+    _check(metcf.spmm(m, Bt, use_values=False), rp, col, None, M, B)
+
+
+@pytest.mark.parametrize("N", [4, 8, 20, 32, 36, 100, 132, 256, 260, 512, 600])
+def test_window_spmm_widths(cuda, N):
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup("wide_window", N)
+    _check(metcf.spmm(m, Bt), rp, col, val, M, B)
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+@pytest.mark.parametrize("N", [32, 128, 256])
+def test_balance_spmm_vs_fp64_and_deterministic(cuda, name, N):
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup(name, N)
+    C1 = metcf.spmm_balance(m, Bt)
+    C2 = metcf.spmm_balance(m, Bt)
+    _check(C1, rp, col, val, M, B)
+    assert (C1.view(-1).view(dtype=__import__("torch").int32) ==
+            C2.view(-1).view(dtype=__import__("torch").int32)).all(), "balance SpMM not bitwise reproducible"
+
+
+@pytest.mark.parametrize("grid", [1, 2, 3, 7, 33, 148, 1000])
+@pytest.mark.parametrize("N", [64, 256, 600])
+def test_schedules_across_many_boundaries(cuda, grid, N):
+    # grid = 1 drives one CTA around its stage ring many times (every
+    # barrier phase is reused); larger grids cut windows across CTAs
+    from dtc_b200 import metcf, B_F32, PREC_TF32
+    for name in ("hub", "banded_dense"):
+        rp, col, val, M, m, B, Bt = _setup(name, N)
+        C = metcf.spmm_ex(m, [Bt], B_F32, N, PREC_TF32, mode=1, grid=grid)
+        _check(C, rp, col, val, M, B)
+        Cw = metcf.spmm_ex(m, [Bt], B_F32, N, PREC_TF32, mode=0, grid=grid)
+        _check(Cw, rp, col, val, M, B)
+    assert metcf.device_status(clear=True) == 0
+
+
+def test_empty_windows_are_zeroed(cuda):
+    import torch
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup("empty_windows", 32)
+    for fn in (metcf.spmm, metcf.spmm_balance):
+        out = torch.full((M, 32), float("nan"), device="cuda")
+        C = fn(m, Bt, out=out)
+        assert torch.isfinite(C).all()
+        assert (C[16:48] == 0).all()
+        _check(C, rp, col, val, M, B)
+
+
+def test_all_ones_known_answer(cuda):
+    import torch
+    from dtc_b200 import metcf
+    rp, col, val, M = cases.duplicates()
+    m = metcf.convert(rp, col, M)
+    X = torch.ones((M, 16), device="cuda")
+    deg = np.array([len(set(col[rp[i]:rp[i + 1]])) for i in range(M)], np.float32)
+    for C in (metcf.spmm(m, X), metcf.spmm_balance(m, X), metcf.spmm_mma_sync(m, X)):
+        np.testing.assert_array_equal(C.cpu().numpy(), np.repeat(deg[:, None], 16, axis=1))
+
+
+@pytest.mark.parametrize("N", [1, 5, 16, 33, 128, 300])
+def test_mma_sync_kernel(cuda, N):
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup("small_uniform", N)
+    _check(metcf.spmm_mma_sync(m, Bt), rp, col, val, M, B)
+
+
+@pytest.mark.parametrize("name", [n for n in cases.CASES])
+def test_against_reference_spmm_golden(cuda, name):
+    import torch
+    from dtc_b200 import metcf
+    path = os.path.join(GOLDEN, f"ref_gpu_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip("no reference golden vector")
+    g = np.load(path)
+    if "C_run" not in g.files:
+        pytest.skip("reference SpMM not run on this case (num_nodes % 16 != 0)")
+    rp, col, _, M = cases.CASES[name]()
+    m = metcf.convert(rp, col, M)
+    Bt = torch.from_numpy(g["B"]).cuda()
+    bound = O.spmm_absbound_f64(rp, col, None, M, g["B"])
+    # The reference's balance launcher runs its atomicAdd-flushing kernel
+    # EXE_TIME = 1000 times into one zero-filled output
+    # (DTC-SpMM/DTCSpMM_kernel.cu:1118-1160, flush at :4885-4900), so the C it
+    # returns is 1000 * A*B (summed in fp32); the window launcher overwrites.
+    ref_balance = g["C_balance"].astype(np.float64) / 1000.0
+    for ours in (metcf.spmm(m, Bt), metcf.spmm_balance(m, Bt)):
+        o = ours.cpu().numpy().astype(np.float64)
+        # both sides are TF32 products of the same operands
+        assert (np.abs(o - g["C_run"]) <= 2 * TF32_TOL * bound + 1e-6).all(), "C_run"
+        assert (np.abs(o - ref_balance) <= (2 * TF32_TOL + 1e-4) * bound + 1e-5).all(), \
+            "C_balance"
+
+
+def test_extension_api_matches_c_abi(cuda):
+    import torch
+    import DTCSpMM
+    from dtc_b200 import metcf
+    rp, col, val, M, m, B, Bt = _setup("hub", 128)
+    ref_w = metcf.spmm(m, Bt, use_values=False)
+    ref_b = metcf.spmm_balance(m, Bt, use_values=False)
+    for plan in ("float_nonsplit", "float4_split", "float2_split"):
+        C = DTCSpMM.run_DTCSpMM(Bt, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                                m.SparseAToX, M, len(col), plan)[0]
+        assert torch.equal(C, ref_w)
+    C = DTCSpMM.DTCSpMM_gcn(Bt, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                            m.SparseAToX, M, len(col))[0]
+    assert torch.equal(C, ref_w)
+    for plan in ("float_nonsplit", "float4_split"):
+        C = DTCSpMM.run_DTCSpMM_balance(Bt, m.TCblockRowid, m.TCblocktileId, m.TCblockoffset,
+                                        m.SparseAToX, M, plan)[0]
+        assert torch.equal(C, ref_b)
+    Cv = DTCSpMM.run_DTCSpMM(Bt, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                             m.SparseAToX, M, len(col), "float_nonsplit", values=m.TCvalues)[0]
+    assert torch.equal(Cv, metcf.spmm(m, Bt))
+    with pytest.raises(RuntimeError):
+        DTCSpMM.run_DTCSpMM(Bt, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                            m.SparseAToX, M, len(col), "float8_magic")
+
+
+def test_no_device_errors_recorded(cuda):
+    from dtc_b200 import metcf
+    assert metcf.device_status(clear=True) == 0
