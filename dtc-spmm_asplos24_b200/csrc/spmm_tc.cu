@@ -1,31 +1,36 @@
-// TC-block SpMM on sm_100a: TMA tile::gather4 of dense rows into 128-byte
-// swizzled shared memory, tcgen05.mma into TMEM, warp-specialised persistent
-// CTAs, deterministic strict balance.
+// TC-block SpMM on sm_100a: cp.async gathers of dense rows into swizzled
+// shared memory, tcgen05.mma into TMEM, warp-specialised persistent CTAs,
+// deterministic strict balance.
 //
 // Product mapping. The reference multiplies each 16x8 TC block A_b (rows of a
 // row window x compacted column slots) by the 8 gathered rows of B with
 // mma.sync m16n8k8 (DTC-SpMM/DTCSpMM_kernel.cu:2776-2794). tcgen05 needs
 // M in {64,128}, so the product is transposed:
 //     C_w^T [features x 16] += B_b^T [features x 8] * A_b^T [8 x 16]
-// UMMA M = 128 features (one N-tile), N = 16 window rows, K = 8 slots (tf32)
-// or 16 (bf16: hi rows + lo rows). Operand "A" of the UMMA is the gathered
-// B rows, which land MN-major (features contiguous) straight from the TMA
-// gather; operand "B" is the densified TC block, K-major, built by warps.
+// UMMA M = 128 features (one N-tile), N = 16 window rows, K = 8 slots. The
+// UMMA "A" operand is the gathered B rows, stored MN-major (features
+// contiguous); the UMMA "B" operand is the densified TC block, K-major.
 // kind::tf32 reads an MN-major operand only in the 128-byte swizzle with
-// 32-byte granules (layout type 1; 16-byte granules read as zeros), which
-// the TMA produces with CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.
+// 32-byte granules (UMMA layout type 1: atoms of 32 features x 4 rows; with
+// 16-byte granules it reads zeros); the loaders write that layout directly.
 //
 // Work split. CTA c owns TC blocks [c*T/G, (c+1)*T/G) (strict balance) or
 // that range snapped to row-window starts (window mode). Windows cut by a
 // CTA boundary write fp32 partial tiles to a workspace; k_reduce_partials
 // sums them in CTA order, so results do not depend on timing.
 //
-// Warp roles (320 threads):
-//   warps 0-3  epilogue: tcgen05.ld 32x32b, coalesced stores of C rows
-//   warp  4    producer: SparseAToX prefetch, TMA gather4 issue
-//   warp  5    TMEM allocator + single-thread UMMA issuer
-//   warps 6-9  tile builders: zero + scatter TC-block values into A_b^T
-#include <cudaTypedefs.h>
+// Pipeline. A ring of S stages, each holding P consecutive TC blocks of the
+// CTA's range (barrier traffic is per stage, not per block).
+//   warps 0-3   epilogue: tcgen05.ld 32x32b, coalesced stores of C rows
+//   warp  4     TMEM allocator + single-thread UMMA issuer
+//   warps 5-8   loaders: cp.async 16-byte gathers of B rows (SparseAToX),
+//               zero-fill for padded slots; stage s is owned by loader s % 4
+//   warps 9-12  tile builders: zero + scatter TC-block values into A_b^T;
+//               stage s is owned by tile builder s % 4
+// Each warp owns a fixed residue class of stages, so it waits on every
+// barrier phase of its stages in order (a parity wait more than one phase
+// ahead would pass spuriously). Every wait is bounded (2 s) and records
+// kErrWaitTimeout instead of hanging.
 #include <cuda_bf16.h>
 #include "common.cuh"
 
@@ -33,11 +38,12 @@ namespace dtc {
 namespace {
 
 constexpr int kEpiWarps = 4;
-constexpr int kProdWarp = 4;
-constexpr int kMmaWarp = 5;
-constexpr int kTileWarp0 = 6;
+constexpr int kMmaWarp = 4;
+constexpr int kLoadWarp0 = 5;
+constexpr int kLoadWarps = 4;
+constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;
 constexpr int kTileWarps = 4;
-constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 320
+constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 416
 constexpr int kNacc = 4;        // TMEM accumulator buffers in flight
 constexpr int kWinH = 16;       // row-window height (BLK_H)
 constexpr int kBlkW = 8;        // TC-block width (BLK_W)
@@ -50,10 +56,11 @@ struct Params {
   const int32_t* toff;       // TCblockoffset [T+1]
   const int32_t* s2x;        // SparseAToX [T*8]
   const float* vals;         // tile-order values or null (A = 1)
+  const float* B;            // [M x N] fp32
   float* C;                  // [M x N]
   float* part;               // partial tiles [2*G x 16 x N] (balance mode)
   uint32_t* err;
-  int32_t M, nwin, N, G, mode, nchunks;  // nchunks: 32-feature chunks per CTA slice
+  int32_t M, nwin, N, G, mode;
   int64_t T;
 };
 
@@ -83,7 +90,8 @@ __device__ __forceinline__ void cta_range(const Params& p, int c, int64_t& b0, i
 }
 
 // Windows walked by a CTA: [w_start, w_end). Empty windows in the range are
-// owned by this CTA (their C rows are zeroed here).
+// owned by this CTA (their C rows are zeroed here); nonempty windows whose
+// intersection with [b0, b1) is empty are skipped.
 __device__ __forceinline__ void cta_windows(const Params& p, int c, int64_t b0, int64_t b1,
                                             int32_t& w_start, int32_t& w_end) {
   int32_t wl = lower_bound_i32(p.rwo, p.nwin, b0);
@@ -100,43 +108,63 @@ __device__ __forceinline__ uint32_t y_offset(uint32_t pos) {
   return (r & 7) * 16 + (r >> 3) * 256 + (s >> 2) * 128 + (s & 3) * 4;
 }
 
-template <int NT, int S>
-struct Smem {
-  static constexpr int kX = S * NT * kXTileBytes;
-  static constexpr int kY = S * kYBytes;
-  static constexpr int kBars = (4 * S + 2 * kNacc) * 8;
-  static constexpr int kTotal = kX + kY + kBars + 16 + 1024;  // + alignment slack
+// Byte offset, inside one 8-row x 128-feature fp32 tile, of 16-byte chunk
+// `cc` (features 4cc..4cc+3) of row k, in the UMMA layout-type-1 atom order:
+// atom = 32 features x 4 rows (512 B), 32-byte granule index XOR (row & 3).
+__device__ __forceinline__ uint32_t x_offset_tf32(uint32_t k, uint32_t cc) {
+  const uint32_t a = cc >> 3, j = cc & 7;
+  const uint32_t g = (j >> 1) ^ (k & 3);
+  return a * 1024 + (k >> 2) * 512 + (k & 3) * 128 + ((g << 1) | (j & 1)) * 16;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int NT, int P, int S>
+struct Cfg {
+  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0, "stage ownership");
+  static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
+  static constexpr int kStageX = P * NT * kXTileBytes;
+  static constexpr int kStageY = P * kYBytes;
+  static constexpr int kX = S * kStageX;
+  static constexpr int kY = S * kStageY;
+  static constexpr int kBars = (2 * S + 2 * kNacc) * 8;
+  static constexpr int kSmem = kX + kY + kBars + 16 + 1024;  // + alignment slack
+  static constexpr uint32_t kTmemCols = (kNacc * NT * 16 <= 32) ? 32 : (kNacc * NT * 16 <= 64) ? 64
+                                        : (kNacc * NT * 16 <= 128) ? 128 : 256;
 };
 
-template <int NT, int S>
-__global__ void __launch_bounds__(kThreads, 1)
-    k_spmm_tf32(const __grid_constant__ CUtensorMap tmapB, const Params p) {
+template <int NT, int P, int S>
+__global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
+  using K = Cfg<NT, P, S>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* xring = smem;
-  uint8_t* yring = smem + Smem<NT, S>::kX;
-  uint64_t* bars = (uint64_t*)(yring + Smem<NT, S>::kY);
-  uint64_t* tma_full = bars;            // [S] producer expect_tx + TMA bytes
-  uint64_t* tile_full = bars + S;       // [S] one tile-builder arrive
-  uint64_t* empty = bars + 2 * S;       // [S] UMMA commit
-  uint64_t* acc_full = bars + 4 * S;    // [kNacc] UMMA commit
+  uint8_t* yring = smem + K::kX;
+  uint64_t* bars = (uint64_t*)(yring + K::kY);
+  uint64_t* full = bars;                 // [S] 32 cp.async arrivals + 1 tile arrival
+  uint64_t* empty = bars + S;            // [S] UMMA commit
+  uint64_t* acc_full = bars + 2 * S;     // [kNacc] UMMA commit
   uint64_t* acc_empty = acc_full + kNacc;  // [kNacc] 4 epilogue warps
   uint32_t* tmem_slot = (uint32_t*)(acc_empty + kNacc);
   volatile uint32_t* abort_flag = tmem_slot + 1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int c = blockIdx.x;
-  const int slice = blockIdx.y;               // 128*NT-feature column slice
-  const int col0 = slice * NT * 128;
-  int nch = p.nchunks - slice * NT * 4;       // chunks in this slice
-  if (nch > NT * 4) nch = NT * 4;
-  constexpr uint32_t kTmemCols = (kNacc * NT * 16 <= 32) ? 32 : (kNacc * NT * 16 <= 64) ? 64
-                                 : (kNacc * NT * 16 <= 128) ? 128 : 256;
+  const int col0 = blockIdx.y * NT * 128;      // this CTA's feature slice
+  const int ncols = (p.N - col0) < NT * 128 ? (p.N - col0) : NT * 128;
+  const int nck = ncols >> 2;                  // 16-byte chunks per gathered row
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
-      mbar_init(&tma_full[i], 1);
-      mbar_init(&tile_full[i], 1);
+      mbar_init(&full[i], 32 + 1);
       mbar_init(&empty[i], 1);
     }
     for (int i = 0; i < kNacc; ++i) {
@@ -147,10 +175,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     fence_mbar_init();
   }
   if (warp == kMmaWarp) {
-    tmem_alloc(tmem_slot, kTmemCols);
+    tmem_alloc(tmem_slot, K::kTmemCols);
     tmem_relinquish();
   }
-  if (warp == kProdWarp && lane == 0) prefetch_tensormap(&tmapB);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -159,101 +186,87 @@ __global__ void __launch_bounds__(kThreads, 1)
   int64_t b0, b1;
   cta_range(p, c, b0, b1);
   const int64_t nblk = b1 - b0;
+  const int64_t nstage = (nblk + P - 1) / P;
 
-  if (warp == kProdWarp) {
-    // ---------------------------------------------------------------- TMA
-    const uint32_t bytes = (uint32_t)nch * 2u * 512u;
-    int4 rows_lo = make_int4(0, 0, 0, 0), rows_hi = rows_lo;  // block b0+32g+lane
-    int4 nxt_lo = rows_lo, nxt_hi = rows_lo;
-    auto load_group = [&](int64_t g, int4& lo, int4& hi) {
-      int64_t b = b0 + g * 32 + lane;
-      if (b < b1) {
-        const int4* q = reinterpret_cast<const int4*>(p.s2x + b * kBlkW);
-        lo = __ldg(q);
-        hi = __ldg(q + 1);
-      }
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
+    // ------------------------------------------------------------ loaders
+    const int lw = warp - kLoadWarp0;
+    auto row_of = [&](int64_t st) -> int32_t {  // SparseAToX entry of this lane
+      const int64_t b = b0 + st * P + (lane >> 3);
+      return (lane < P * kBlkW && st < nstage && b < b1) ? __ldg(p.s2x + b * kBlkW + (lane & 7))
+                                                         : 0;
     };
-    if (nblk > 0) load_group(0, nxt_lo, nxt_hi);
-    for (int64_t i = 0; i < nblk; ++i) {
-      const int j = (int)(i & 31);
-      if (j == 0) {
-        rows_lo = nxt_lo;
-        rows_hi = nxt_hi;
-        if (i + 32 < nblk) load_group((i >> 5) + 1, nxt_lo, nxt_hi);
-      }
-      const int s = (int)(i % S);
-      const uint32_t n = (uint32_t)(i / S);
+    int32_t rows = row_of(lw);
+    for (int64_t st = lw; st < nstage; st += kLoadWarps) {
+      const int s = (int)(st % S);
+      const uint32_t n = (uint32_t)(st / S);
+      const int32_t nxt = row_of(st + kLoadWarps);  // prefetch this warp's next stage
       const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
       if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
-      int32_t r[8];
-      r[0] = __shfl_sync(0xffffffffu, rows_lo.x, j);
-      r[1] = __shfl_sync(0xffffffffu, rows_lo.y, j);
-      r[2] = __shfl_sync(0xffffffffu, rows_lo.z, j);
-      r[3] = __shfl_sync(0xffffffffu, rows_lo.w, j);
-      r[4] = __shfl_sync(0xffffffffu, rows_hi.x, j);
-      r[5] = __shfl_sync(0xffffffffu, rows_hi.y, j);
-      r[6] = __shfl_sync(0xffffffffu, rows_hi.z, j);
-      r[7] = __shfl_sync(0xffffffffu, rows_hi.w, j);
-      // padded slots (always after slot 0, column id 0) -> out-of-range row: zero fill
+      const int64_t sb = b0 + st * P;
+      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      const uint32_t xs = smem_u32(xring + (size_t)s * K::kStageX);
+      for (int pb = 0; pb < nb; ++pb) {
 #pragma unroll
-      for (int k = 1; k < 8; ++k)
-        if (r[k] == 0) r[k] = p.M;
-      if (lane == 0) mbar_arrive_expect_tx(&tma_full[s], bytes);
-      __syncwarp();
-      uint8_t* xs = xring + (size_t)s * NT * kXTileBytes;
-      for (int o = lane; o < 2 * nch; o += 32) {
-        const int h = o & 1, ch = o >> 1;
-        uint8_t* dst = xs + ch * 1024 + h * 512;
-        tma_gather4(dst, &tmapB, &tma_full[s], col0 + ch * 32, r[4 * h + 0], r[4 * h + 1],
-                    r[4 * h + 2], r[4 * h + 3]);
+        for (int k = 0; k < kBlkW; ++k) {
+          const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+          const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
+          const float* src = p.B + (int64_t)(pad ? 0 : r) * p.N + col0;
+          for (int cc = lane; cc < nck; cc += 32) {
+            const int t = cc >> 5;
+            cp_async16(xs + (pb * NT + t) * kXTileBytes + x_offset_tf32(k, cc & 31), src + cc * 4,
+                       pad ? 0u : 16u);
+          }
+        }
       }
+      cp_async_arrive_noinc(&full[s]);
+      rows = nxt;
     }
   } else if (warp >= kTileWarp0) {
     // ------------------------------------------------------ tile builders
-    // Warp tw owns ring stages [tw*kBatch, (tw+1)*kBatch) in every round, so
-    // each warp waits on its stages' `empty` phases strictly in order (a
-    // parity wait more than one phase ahead would pass spuriously).
-    constexpr int kBatch = S / kTileWarps;
-    static_assert(S % kTileWarps == 0 && kBatch >= 1 && kBatch <= 31, "ring split");
     const int tw = warp - kTileWarp0;
-    for (int64_t bb = b0 + (int64_t)tw * kBatch; bb < b1; bb += (int64_t)S) {
-      const int nb = (int)((b1 - bb) < kBatch ? (b1 - bb) : kBatch);
-      int32_t offv = (lane <= nb) ? __ldg(p.toff + bb + lane) : 0;
-      int32_t off[kBatch + 1];
+    auto offs_of = [&](int64_t st) -> int32_t {
+      const int64_t sb = b0 + st * P;
+      return (st < nstage && lane <= P && sb + lane <= b1) ? __ldg(p.toff + sb + lane) : 0;
+    };
+    int32_t offv = offs_of(tw);
+    for (int64_t st = tw; st < nstage; st += kTileWarps) {
+      const int s = (int)(st % S);
+      const uint32_t n = (uint32_t)(st / S);
+      const int32_t nxt = offs_of(st + kTileWarps);
+      const int64_t sb = b0 + st * P;
+      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      int32_t off[P + 1];
 #pragma unroll
-      for (int k = 0; k <= kBatch; ++k) off[k] = __shfl_sync(0xffffffffu, offv, k);
-      // wait for the batch's stages, zero their A tiles
-      bool ok = true;
-      for (int k = 0; k < nb; ++k) {
-        const int64_t i = bb + k - b0;
-        const int s = (int)(i % S);
-        const uint32_t n = (uint32_t)(i / S);
-        const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
-        if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
-        float4* y = reinterpret_cast<float4*>(yring + (size_t)s * kYBytes);
-        y[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-      if (!__all_sync(0xffffffffu, ok && !*abort_flag)) { *abort_flag = 1; break; }
+      for (int k = 0; k <= P; ++k) off[k] = __shfl_sync(0xffffffffu, offv, k);
+      const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
+      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      uint8_t* ys = yring + (size_t)s * K::kStageY;
+#pragma unroll
+      for (int z = lane; z < P * kYBytes / 16; z += 32)
+        reinterpret_cast<float4*>(ys)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncwarp();
       const int32_t e0 = off[0], e1 = off[nb];
       for (int32_t e = e0 + lane; e < e1; e += 32) {
-        int k = 0;
+        int pb = 0;
 #pragma unroll
-        for (int q = 1; q < kBatch; ++q) k += (q < nb && e >= off[q]) ? 1 : 0;
+        for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
         const uint32_t pos = __ldg(p.tile + e);
-        float v = p.vals ? __ldg(p.vals + e) : 1.0f;
-        if (pos < kWinH * kBlkW && v != 0.0f) {
-          uint32_t t32;
-          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t32) : "f"(v));
-          const int s = (int)((bb + k - b0) % S);
-          *reinterpret_cast<uint32_t*>(yring + (size_t)s * kYBytes + y_offset(pos)) = t32;
-        } else if (pos >= kWinH * kBlkW) {
+        const float v = p.vals ? __ldg(p.vals + e) : 1.0f;
+        if (pos < kWinH * kBlkW) {
+          if (v != 0.0f) {
+            uint32_t t32;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t32) : "f"(v));
+            *reinterpret_cast<uint32_t*>(ys + pb * kYBytes + y_offset(pos)) = t32;
+          }
+        } else {
           atomicOr(p.err, kErrBadIndex);
         }
       }
       fence_proxy_async_smem();
       __syncwarp();
-      if (lane == 0)
-        for (int k = 0; k < nb; ++k) mbar_arrive(&tile_full[(int)((bb + k - b0) % S)]);
+      if (lane == 0) mbar_arrive(&full[s]);
+      offv = nxt;
     }
   } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------- UMMA
@@ -262,36 +275,35 @@ __global__ void __launch_bounds__(kThreads, 1)
       cta_windows(p, c, b0, b1, ws, we);
       constexpr uint32_t idesc = umma_idesc(2, 128, 16, 1, 0);
       const uint32_t xbase = smem_u32(xring), ybase = smem_u32(yring);
-      int64_t i = 0;  // block counter within the CTA range
-      uint32_t q = 0;  // segment counter
+      int64_t cur = -1;  // stage whose `full` phase has been consumed
+      uint32_t q = 0;    // segment counter
       bool ok = true;
       for (int32_t w = ws; w < we && ok; ++w) {
         const int64_t r0 = __ldg(p.rwo + w), r1 = __ldg(p.rwo + w + 1);
-        if (r0 == r1) continue;
         const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
+        if (s0 >= s1) continue;  // empty window, or no blocks of it in this range
         const int a = (int)(q % kNacc);
         if (!mbar_wait(&acc_empty[a], ((q / kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
         tc_fence_after();
-        for (int64_t b = s0; b < s1; ++b, ++i) {
-          const int s = (int)(i % S);
-          const uint32_t n = (uint32_t)(i / S);
-          if (!mbar_wait(&tma_full[s], n & 1, p.err) || !mbar_wait(&tile_full[s], n & 1, p.err)) {
-            ok = false;
-            break;
+        for (int64_t b = s0; b < s1; ++b) {
+          const int64_t i = b - b0, st = i / P;
+          const int pb = (int)(i - st * P);
+          const int s = (int)(st % S);
+          if (st != cur) {
+            if (!mbar_wait(&full[s], (uint32_t)(st / S) & 1, p.err)) { ok = false; break; }
+            fence_proxy_async_smem();  // cp.async (generic proxy) data -> UMMA reads
+            tc_fence_after();
+            cur = st;
           }
-          tc_fence_after();
-          const uint64_t bdesc = umma_desc(ybase + s * kYBytes, 128, 256, 0);
+          const uint64_t bdesc = umma_desc(ybase + s * K::kStageY + pb * kYBytes, 128, 256, 0);
 #pragma unroll
           for (int t = 0; t < NT; ++t) {
-            // MN-major tf32 operands use the 128-byte swizzle with 32-byte
-            // granules (UMMA layout type 1): atoms of 32 features x 4 rows;
-            // LBO = 1024 B between 32-feature atoms, SBO = 512 B between the
-            // two 4-row halves -- exactly where the two gather4 ops land.
-            const uint64_t adesc = umma_desc(xbase + (s * NT + t) * kXTileBytes, 1024, 512, 1);
+            const uint64_t adesc =
+                umma_desc(xbase + s * K::kStageX + (pb * NT + t) * kXTileBytes, 1024, 512, 1);
             mma_tf32(tmem_base + (uint32_t)((a * NT + t) * 16), adesc, bdesc, idesc,
                      b == s0 ? 0u : 1u);
           }
-          tc_commit(&empty[s]);
+          if (pb == P - 1 || b == b1 - 1) tc_commit(&empty[s]);
         }
         if (!ok) break;
         tc_commit(&acc_full[a]);
@@ -310,16 +322,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int64_t r0 = __ldg(p.rwo + w), r1 = __ldg(p.rwo + w + 1);
       const int64_t row0 = (int64_t)w * kWinH;
       if (r0 == r1) {  // empty window: C rows are zero
-        for (int f = col0 + ew * 32 + lane; f < p.N && f < col0 + NT * 128; f += 128)
+        for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
           for (int r = 0; r < kWinH && row0 + r < p.M; ++r) p.C[(row0 + r) * p.N + f] = 0.0f;
         continue;
       }
+      if ((r0 > b0 ? r0 : b0) >= (r1 < b1 ? r1 : b1)) continue;
       const int a = (int)(q % kNacc);
       const bool got = mbar_wait(&acc_full[a], (q / kNacc) & 1, p.err);
       if (!__all_sync(0xffffffffu, got)) { *abort_flag = 1; break; }
       tc_fence_after();
       float* out;
-      int64_t ld;
       bool guard_rows = true;
       if (p.mode == 1 && (r0 < b0 || r1 > b1)) {  // window cut by a CTA boundary
         const int slot = (r0 < b0) ? 2 * c : 2 * c + 1;
@@ -328,7 +340,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       } else {
         out = p.C + row0 * p.N;
       }
-      ld = p.N;
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
         uint32_t v[16];
@@ -343,7 +354,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (f < p.N) {
 #pragma unroll
           for (int r = 0; r < kWinH; ++r)
-            if (!guard_rows || row0 + r < p.M) out[r * ld + f] = __uint_as_float(v[r]);
+            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = __uint_as_float(v[r]);
         }
       }
       ++q;
@@ -354,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   if (warp == kMmaWarp) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, kTmemCols);
+    tmem_dealloc(tmem_base, K::kTmemCols);
   }
 }
 
@@ -399,58 +410,20 @@ __global__ void k_rowid_to_rwo(const int32_t* __restrict__ rowid, int64_t T, int
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void* ptr = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)ptr;
-  }
-  return fn;
-}
-
-// 2-D map over a row-major [rows x N] matrix of `esize`-byte elements, box =
-// 128 bytes x 1 row, 128-byte swizzle. 4-byte elements use 32-byte swizzle
-// granules (the layout UMMA kind::tf32 reads MN-major), 2-byte elements the
-// 16-byte granules of the standard 128-byte swizzle.
-dtc_status make_row_map(CUtensorMap* map, const void* base, CUtensorMapDataType dt, int esize,
-                        int64_t rows, int32_t N) {
-  auto enc = get_encode();
-  if (!enc) {
-    set_error("cuTensorMapEncodeTiled unavailable");
-    return DTC_ERR_UNSUPPORTED;
-  }
-  cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)N * esize};
-  cuuint32_t box[2] = {(cuuint32_t)(128 / esize), 1};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = enc(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   esize == 4 ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
-    return DTC_ERR_CUDA;
-  }
-  return DTC_OK;
-}
-
-template <int NT, int S>
-dtc_status launch_tf32(const CUtensorMap& map, const Params& p, int slices, cudaStream_t st) {
-  constexpr int smem = Smem<NT, S>::kTotal;
+template <int NT, int P, int S>
+dtc_status launch_tf32(const Params& p, int slices, cudaStream_t st) {
+  constexpr int smem = Cfg<NT, P, S>::kSmem;
+  static_assert(smem <= 227 * 1024, "shared memory budget");
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    DTC_CUDA(cudaFuncSetAttribute(k_spmm_tf32<NT, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  smem));
+    DTC_CUDA(cudaFuncSetAttribute(k_spmm_tf32<NT, P, S>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set[dev & 63] = true;
   }
   dim3 grid((unsigned)p.G, (unsigned)slices);
-  k_spmm_tf32<NT, S><<<grid, kThreads, smem, st>>>(map, p);
+  k_spmm_tf32<NT, P, S><<<grid, kThreads, smem, st>>>(p);
   DTC_CUDA(cudaGetLastError());
   if (p.mode == 1 && p.G > 1) {
     k_reduce_partials<<<p.G - 1, 256, 0, st>>>(p);
@@ -467,7 +440,7 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
                           float* part, cudaStream_t st) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
-  DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0 (16-byte TMA row stride)");
+  DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0 (16-byte row segments)");
   DTC_REQUIRE(((uintptr_t)B & 15) == 0, "B must be 16-byte aligned");
   DTC_REQUIRE(nwin == (M + kWinH - 1) / kWinH, "num_windows must be ceil(num_nodes/16)");
   if (!is_sm100()) {
@@ -480,19 +453,15 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
     return DTC_OK;
   }
   Params p{};
-  p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals;
+  p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals; p.B = B;
   p.C = C; p.part = part; p.err = device_error_word();
   p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
   int G = grid > 0 ? grid : num_sms();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
-  p.nchunks = (N + 31) / 32;
-  CUtensorMap map;
-  dtc_status s = make_row_map(&map, B, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, M, N);
-  if (s != DTC_OK) return s;
-  if (N <= 128) return launch_tf32<1, 32>(map, p, 1, st);
-  if (N <= 256) return launch_tf32<2, 24>(map, p, 1, st);
-  return launch_tf32<4, 12>(map, p, (N + 511) / 512, st);
+  if (N <= 128) return launch_tf32<1, 4, 8>(p, 1, st);
+  if (N <= 256) return launch_tf32<2, 2, 8>(p, 1, st);
+  return launch_tf32<4, 1, 8>(p, (N + 511) / 512, st);
 }
 
 size_t spmm_partials_bytes(int64_t T, int32_t N, int grid) {
