@@ -22,10 +22,15 @@
 // Pipeline. A ring of S stages, each holding P consecutive TC blocks of the
 // CTA's range (barrier traffic is per stage, not per block).
 //   warps 0-3   epilogue: tcgen05.ld 32x32b, coalesced stores of C rows
-//   warp  4     TMEM allocator + single-thread UMMA issuer
-//   warps 5-8   loaders: cp.async 16-byte gathers of B rows (SparseAToX),
+//   warps 4-5   UMMA issuers (one thread each; warp 4 also owns TMEM):
+//               issuer m takes the stages s % 2 == m into its own set of
+//               accumulators, so two MMA streams are in flight (a single
+//               issuing thread cannot saturate the tensor pipe with these
+//               small M128 x N16 x K8 instructions); the epilogue adds the
+//               two partial accumulators in a fixed order
+//   warps 6-9   loaders: cp.async 16-byte gathers of B rows (SparseAToX),
 //               zero-fill for padded slots; stage s is owned by loader s % 4
-//   warps 9-12  tile builders: zero + scatter TC-block values into A_b^T;
+//   warps 10-13 tile builders: zero + scatter TC-block values into A_b^T;
 //               stage s is owned by tile builder s % 4
 // Each warp owns a fixed residue class of stages, so it waits on every
 // barrier phase of its stages in order (a parity wait more than one phase
@@ -38,12 +43,13 @@ namespace dtc {
 namespace {
 
 constexpr int kEpiWarps = 4;
-constexpr int kMmaWarp = 4;
-constexpr int kLoadWarp0 = 5;
+constexpr int kMmaWarp = 4;     // UMMA issuers: warps 4 and 5 (lane 0 each)
+constexpr int kMmaWarps = 2;
+constexpr int kLoadWarp0 = kMmaWarp + kMmaWarps;
 constexpr int kLoadWarps = 4;
 constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;
 constexpr int kTileWarps = 4;
-constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 416
+constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 448
 constexpr int kNacc = 4;        // TMEM accumulator buffers in flight
 constexpr int kWinH = 16;       // row-window height (BLK_H)
 constexpr int kBlkW = 8;        // TC-block width (BLK_W)
@@ -129,7 +135,8 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
 
 template <int NT, int P, int S>
 struct Cfg {
-  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0, "stage ownership");
+  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kMmaWarps == 0,
+                "stage ownership");
   static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
   static constexpr int kStageX = P * NT * kXTileBytes;
   static constexpr int kStageY = P * kYBytes;
@@ -137,8 +144,10 @@ struct Cfg {
   static constexpr int kY = S * kStageY;
   static constexpr int kBars = (2 * S + 2 * kNacc) * 8;
   static constexpr int kSmem = kX + kY + kBars + 16 + 1024;  // + alignment slack
-  static constexpr uint32_t kTmemCols = (kNacc * NT * 16 <= 32) ? 32 : (kNacc * NT * 16 <= 64) ? 64
-                                        : (kNacc * NT * 16 <= 128) ? 128 : 256;
+  static constexpr int kCols = kMmaWarps * kNacc * NT * 16;  // TMEM columns used
+  static_assert(kCols <= 512, "TMEM budget");
+  static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
+                                        : kCols <= 256 ? 256 : 512;
 };
 
 template <int NT, int P, int S>
@@ -168,7 +177,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       mbar_init(&empty[i], 1);
     }
     for (int i = 0; i < kNacc; ++i) {
-      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_full[i], kMmaWarps);
       mbar_init(&acc_empty[i], kEpiWarps);
     }
     *abort_flag = 0;
@@ -268,45 +277,61 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       if (lane == 0) mbar_arrive(&full[s]);
       offv = nxt;
     }
-  } else if (warp == kMmaWarp) {
+  } else if (warp >= kMmaWarp && warp < kMmaWarp + kMmaWarps) {
     // ------------------------------------------------------------- UMMA
     if (lane == 0) {
+      const int m = warp - kMmaWarp;  // this issuer's stages: st % kMmaWarps == m
       int32_t ws, we;
       cta_windows(p, c, b0, b1, ws, we);
       constexpr uint32_t idesc = umma_idesc(2, 128, 16, 1, 0);
-      const uint32_t xbase = smem_u32(xring), ybase = smem_u32(yring);
-      int64_t cur = -1;  // stage whose `full` phase has been consumed
-      uint32_t q = 0;    // segment counter
+      // Descriptors advance by adding (byte offset >> 4) to the start-address
+      // field (shared addresses < 256 KB fit its 14 bits, no carry out).
+      const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 512, 1);
+      const uint64_t bdesc0 = umma_desc(smem_u32(yring), 128, 256, 0);
+      uint32_t q = 0;        // segment counter
       bool ok = true;
+      int64_t r0 = ws < we ? __ldg(p.rwo + ws) : 0;
+      int64_t r1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
       for (int32_t w = ws; w < we && ok; ++w) {
-        const int64_t r0 = __ldg(p.rwo + w), r1 = __ldg(p.rwo + w + 1);
+        const int64_t r2 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;  // next window's end
         const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
+        r0 = r1;
+        r1 = r2;
         if (s0 >= s1) continue;  // empty window, or no blocks of it in this range
         const int a = (int)(q % kNacc);
         if (!mbar_wait(&acc_empty[a], ((q / kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
         tc_fence_after();
-        for (int64_t b = s0; b < s1; ++b) {
-          const int64_t i = b - b0, st = i / P;
-          const int pb = (int)(i - st * P);
+        const uint32_t dtm = tmem_base + (uint32_t)((m * kNacc + a) * NT * 16);
+        uint32_t acc = 0;
+        // this issuer's stages that intersect [s0, s1)
+        int64_t st = (s0 - b0) / P;
+        st += (m - (int)(st % kMmaWarps) + kMmaWarps) % kMmaWarps;
+        const int64_t st_last = (s1 - 1 - b0) / P;
+        for (; st <= st_last; st += kMmaWarps) {
           const int s = (int)(st % S);
-          if (st != cur) {
+          const int64_t sb = b0 + st * P;                 // first block of stage st
+          const int64_t lo = sb > s0 ? sb : s0;
+          const int64_t hi = (sb + P) < s1 ? (sb + P) : s1;
+          if (lo == sb) {  // first visit of this stage (segments are walked in order)
             if (!mbar_wait(&full[s], (uint32_t)(st / S) & 1, p.err)) { ok = false; break; }
             fence_proxy_async_smem();  // cp.async (generic proxy) data -> UMMA reads
             tc_fence_after();
-            cur = st;
           }
-          const uint64_t bdesc = umma_desc(ybase + s * K::kStageY + pb * kYBytes, 128, 256, 0);
+          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * kYBytes) >> 4);
+          uint64_t adesc =
+              adesc0 + (uint64_t)((s * K::kStageX + (int)(lo - sb) * NT * kXTileBytes) >> 4);
+          for (int64_t b = lo; b < hi; ++b) {
 #pragma unroll
-          for (int t = 0; t < NT; ++t) {
-            const uint64_t adesc =
-                umma_desc(xbase + s * K::kStageX + (pb * NT + t) * kXTileBytes, 1024, 512, 1);
-            mma_tf32(tmem_base + (uint32_t)((a * NT + t) * 16), adesc, bdesc, idesc,
-                     b == s0 ? 0u : 1u);
+            for (int t = 0; t < NT; ++t)
+              mma_tf32(dtm + t * 16, adesc + (uint64_t)(t * (kXTileBytes >> 4)), bdesc, idesc, acc);
+            acc = 1;
+            adesc += (uint64_t)((NT * kXTileBytes) >> 4);
+            bdesc += (uint64_t)(kYBytes >> 4);
           }
-          if (pb == P - 1 || b == b1 - 1) tc_commit(&empty[s]);
+          if (hi == sb + P || hi == b1) tc_commit(&empty[s]);  // stage fully consumed
         }
         if (!ok) break;
-        tc_commit(&acc_full[a]);
+        tc_commit(&acc_full[a]);  // also when this issuer had no block in the segment
         ++q;
       }
       if (!ok) *abort_flag = 1;
@@ -318,8 +343,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
     cta_windows(p, c, b0, b1, ws, we);
     const int ew = warp;  // TMEM lanes 32*ew .. 32*ew+31
     uint32_t q = 0;
+    int64_t rn0 = ws < we ? __ldg(p.rwo + ws) : 0;
+    int64_t rn1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
     for (int32_t w = ws; w < we; ++w) {
-      const int64_t r0 = __ldg(p.rwo + w), r1 = __ldg(p.rwo + w + 1);
+      const int64_t r0 = rn0, r1 = rn1;
+      rn0 = rn1;
+      rn1 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;  // prefetch the next window's end
       const int64_t row0 = (int64_t)w * kWinH;
       if (r0 == r1) {  // empty window: C rows are zero
         for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
@@ -340,11 +369,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       } else {
         out = p.C + row0 * p.N;
       }
+      // issuers that hold part of this segment: stages of [s0, s1) mod kMmaWarps
+      const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
+      const int64_t st0 = (s0 - b0) / P, st1 = (s1 - 1 - b0) / P;
+      const bool both = st1 > st0;
+      const int m0 = (int)(st0 % kMmaWarps);
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        uint32_t v[16];
-        tmem_ld16(tmem_base + ((uint32_t)(ew * 32) << 16) + (uint32_t)((a * NT + t) * 16), v);
+        uint32_t v[16], u[16];
+        const uint32_t lane_addr = tmem_base + ((uint32_t)(ew * 32) << 16);
+        tmem_ld16(lane_addr + (uint32_t)(((m0 * kNacc + a) * NT + t) * 16), v);
+        if (both) tmem_ld16(lane_addr + (uint32_t)((((1 - m0) * kNacc + a) * NT + t) * 16), u);
         tmem_ld_wait();
+        float x[16];
+        if (both) {  // fixed order: issuer 0's partial + issuer 1's partial
+#pragma unroll
+          for (int r = 0; r < kWinH; ++r)
+            x[r] = m0 == 0 ? __uint_as_float(v[r]) + __uint_as_float(u[r])
+                           : __uint_as_float(u[r]) + __uint_as_float(v[r]);
+        } else {
+#pragma unroll
+          for (int r = 0; r < kWinH; ++r) x[r] = __uint_as_float(v[r]);
+        }
         const int f = col0 + t * 128 + ew * 32 + lane;
         if (t == NT - 1) {
           tc_fence_before();
@@ -354,7 +400,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
         if (f < p.N) {
 #pragma unroll
           for (int r = 0; r < kWinH; ++r)
-            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = __uint_as_float(v[r]);
+            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = x[r];
         }
       }
       ++q;
