@@ -224,24 +224,43 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from dtc_b200 import metcf
+    from dtc_b200 import metcf, B_F32, B_SPLIT24, B_BF16, B_FP8, PREC_TF32, PREC_SPLIT3, PREC_SPLIT4
     import DTCSpMM
 
     A, Bh, N, name = make_workload(args)
     dev = torch.device("cuda", local)
     m = metcf.convert(A.rowptr, A.col, A.M, values=A.val, device=dev)
     B = torch.from_numpy(Bh).to(dev)
-    Cd = torch.empty((A.M, N), dtype=torch.float32, device=dev)
     flops = 2.0 * A.nnz * N
     peaks, peak_kind = load_peaks()
 
-    # forms measured (same matrix, same B)
+    planes = {B_SPLIT24: metcf.pack_b(B, B_SPLIT24), B_BF16: metcf.pack_b(B, B_BF16),
+              B_FP8: metcf.pack_b(B, B_FP8)}
+    outs = {}
+
+    def out_for(k):
+        if k not in outs:
+            outs[k] = torch.empty((A.M, N), dtype=torch.float32, device=dev)
+        return outs[k]
+
+    wsb = max(metcf.spmm_balance_workspace_bytes(m, N), 1)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+
+    def ex(fmt, prec, mode, k):
+        pl = [B] if fmt == B_F32 else planes[fmt]
+        return lambda: metcf.spmm_ex(m, pl, fmt, N, prec, mode=mode, out=out_for(k),
+                                     workspace=ws)
+
+    # (storage form, precision, schedule) -> bytes per gathered B element
     forms = {
-        "tf32_window": lambda: metcf.spmm(m, B, out=Cd),
-        "tf32_balance": lambda: metcf.spmm_balance(m, B, out=Cd, workspace=ws_bal),
+        "tf32_window": (ex(B_F32, PREC_TF32, 0, "tf32_window"), 4.0, 1),
+        "tf32_balance": (ex(B_F32, PREC_TF32, 1, "tf32_balance"), 4.0, 2),
+        "split24x4_window": (ex(B_SPLIT24, PREC_SPLIT4, 0, "split24x4_window"), 3.0, 1),
+        "split24x4_balance": (ex(B_SPLIT24, PREC_SPLIT4, 1, "split24x4_balance"), 3.0, 2),
+        "split24x3_balance": (ex(B_SPLIT24, PREC_SPLIT3, 1, "split24x3_balance"), 3.0, 2),
+        "bf16_balance": (ex(B_BF16, PREC_SPLIT4, 1, "bf16_balance"), 2.0, 2),
+        "fp8_balance": (ex(B_FP8, PREC_SPLIT4, 1, "fp8_balance"), 1.0 + 4.0 / N, 2),
     }
-    ws_bal = torch.empty(metcf.spmm_balance_workspace_bytes(m, N), dtype=torch.uint8, device=dev)
-    launches = {"tf32_window": 1, "tf32_balance": 3}
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -270,61 +289,75 @@ def main():
         return total / steps, per, wall
 
     results = {}
-    for k, fn in forms.items():
+    for k, (fn, eb, nl) in forms.items():
         ms, per, _ = timed(fn, max(3, args.steps // 2), args.warmup)
-        results[k] = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9}
-    best = min(results, key=lambda k: results[k]["ms"])
+        nbytes = algorithmic_bytes(m, N, eb)[0]
+        results[k] = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9,
+                      "hbm_frac": nbytes / (float(np.mean(per)) * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                      "bytes_per_B_elem": eb}
+    tf32_best = min(("tf32_window", "tf32_balance"), key=lambda k: results[k]["ms"])
+    tuned = min(("split24x4_window", "split24x4_balance"), key=lambda k: results[k]["ms"])
 
-    # headline timed region: K steps of the best form, clocks sampled
+    # headline timed region: K steps of the tuned form, clocks sampled
     with Clocks(local) as clk:
-        ms, per, wall = timed(forms[best], args.steps, args.warmup)
+        ms, per, wall = timed(forms[tuned][0], args.steps, args.warmup)
     clocks = clk.summary()
     value = world * flops / (ms * 1e-3) / 1e9
 
-    nbytes, U, S = algorithmic_bytes(m, N, 4)
+    nbytes, U, S = algorithmic_bytes(m, N, forms[tuned][1])
     kern_ms = float(np.mean(per))
     achieved = nbytes / (kern_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                 "peak_kind": peak_kind, "algorithmic_bytes": nbytes, "distinct_rows_U": U,
-                "metcf_bytes": S, "compulsory_bytes": S + A.K * N * 4 + A.M * N * 4,
-                "kernel": best, "kernel_ms": kern_ms}
+                "metcf_bytes": S, "compulsory_bytes": S + A.K * N * 3 + A.M * N * 4,
+                "kernel": tuned, "kernel_ms": kern_ms}
 
-    # end-to-end through the reference-facing API: pinned host B -> device,
-    # run_DTCSpMM, C -> pinned host
+    # end-to-end through the public API with host buffers: pinned fp32 B ->
+    # device, storage-form pack, SpMM, C -> pinned host
     Bpin = torch.from_numpy(Bh).pin_memory()
     Cpin = torch.empty((A.M, N), dtype=torch.float32).pin_memory()
     Bdev = torch.empty_like(B)
 
     def e2e_step():
         Bdev.copy_(Bpin, non_blocking=True)
-        C = DTCSpMM.run_DTCSpMM(Bdev, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
-                                m.SparseAToX, A.M, A.nnz, "float_nonsplit", values=m.TCvalues)[0]
+        pl = DTCSpMM.pack_b(Bdev, B_SPLIT24)
+        C = DTCSpMM.run_DTCSpMM_ex(pl, B_SPLIT24, N, m.RowWindowOffset, m.TCblocktileId,
+                                   m.TCblockoffset, m.SparseAToX, A.M, PREC_SPLIT4,
+                                   1 if tuned.endswith("balance") else 0, 0,
+                                   values=m.TCvalues)[0]
         Cpin.copy_(C, non_blocking=True)
 
     e2e_steps = max(3, min(args.steps, 10))
     e_ms, _, _ = timed(e2e_step, e2e_steps, 2)
     e2e = {"value": world * flops / (e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
            "h2d_bytes_per_step": int(Bh.nbytes), "d2h_bytes_per_step": int(A.M * N * 4),
-           "api": "DTCSpMM.run_DTCSpMM"}
+           "api": "DTCSpMM.pack_b + DTCSpMM.run_DTCSpMM_ex"}
 
-    cpu, err = (None, None)
+    cpu, errs = (None, {})
     if rank == 0 and world == 1 and not args.no_cpu:
-        forms[best]()
-        torch.cuda.synchronize()
-        cpu, err = cpu_baseline(A, Bh, N, gpu_C=Cd.cpu().numpy())
+        cpu, _ = cpu_baseline(A, Bh, N)
+        for k in (tf32_best, tuned, "split24x3_balance", "bf16_balance", "fp8_balance"):
+            forms[k][0]()
+            torch.cuda.synchronize()
+            errs[k] = accuracy_vs_fp64(A, Bh, N, outs[k].cpu().numpy())
+            results[k]["rel_err_vs_fp64"] = errs[k]["rel_fro"]
+            results[k]["max_abs_err"] = errs[k]["max_abs"]
 
     if rank == 0:
         line = {"metric": "SpMM GFLOP/s (2*nnz*N) & HBM-roofline %", "value": value,
                 "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "tf32", "data": "synthetic",
+                "vs_baseline": None, "dtype": "bf16x2 (split, fp32 accumulate)",
+                "data": "synthetic",
                 "config": {"workload": name, "num_nodes": A.M, "nnz": A.nnz, "N": N,
-                           "T": m.T, "form": best, "l2": "inputs larger than L2 (B 512 MiB,"
-                           " ME-TCF %.0f MB); no flush" % (S / 1e6)},
+                           "T": m.T, "form": tuned, "plain_form": tf32_best,
+                           "l2": "inputs larger than L2 (B %.0f MiB fp32, ME-TCF %.0f MB); no flush"
+                           % (A.K * N * 4 / 2 ** 20, S / 1e6)},
+                "speedup_vs_plain_tf32": results[tf32_best]["ms"] / ms,
                 "forms": results, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
-                "accuracy_vs_fp64": err, "clocks": clocks,
-                "gpu_launches": launches[best] * args.steps}
+                "accuracy_vs_fp64": errs.get(tuned), "clocks": clocks,
+                "gpu_launches": forms[tuned][2] * args.steps}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

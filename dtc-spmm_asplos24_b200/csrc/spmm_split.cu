@@ -1,13 +1,622 @@
-// Split-precision TC-block SpMM (bf16 hi/lo products on tcgen05 kind::f16).
-#include "common.cuh"
+// Split-precision TC-block SpMM: bf16 operands on tcgen05 kind::f16 with
+// fp32 accumulation in TMEM, B gathered from a compact storage form.
+//
+// Forms (B storage, see formats.cu):
+//   SPLIT24 : bf16 hi plane + u8 extension plane (3 bytes/element). The
+//             tile warps rebuild lo = b24 - hi (exact in bf16) in shared
+//             memory, so B_hi + B_lo reproduces B rounded to 16 significant
+//             bits.
+//   BF16    : bf16 plane (2 bytes/element); lo = 0.
+//   FP8     : e4m3 plane + fp32 row scale (1 byte/element); the tile warps
+//             expand q * scale[row] to bf16 hi; lo = 0.
+// A values are split the same way: A_hi = bf16(a), A_lo = bf16(a - A_hi).
+//
+// One UMMA per TC block and 128-feature tile computes every product term:
+//   UMMA A operand (M = 128 features x K = 16): rows k < 8 are B_hi of the
+//   block's 8 gathered rows, rows k >= 8 are B_lo (MN-major, 128-byte swizzle)
+//   UMMA B operand (K = 16 x N = 32, K-major): columns 0..15 hold A_hi^T
+//   (over both K halves), columns 16..31 hold A_lo^T (over the hi half; over
+//   the lo half too for the 4-term form).
+//   D[:, r] + D[:, 16 + r] = (B_hi + B_lo) A_hi^T + (B_hi [+ B_lo]) A_lo^T.
+// The N = 32 instruction costs the same tensor-pipe time as N = 16, so the
+// full product takes one instruction per block, like the tf32 form, while
+// gathering 3 (SPLIT24), 2 (BF16) or 1 (FP8) bytes per element instead of 4.
+//
+// Schedule, work split and the deterministic reduction are the tf32
+// kernel's (spmm_tc.cu). Warp roles (512 threads): epilogue 0-3, UMMA
+// issuers 4-5, loaders 6-7 (cp.async of the planes), tile builders 8-11
+// (A_hi / A_lo tiles), converters 12-15 (wait for a stage's gathered rows,
+// rebuild the bf16 operand rows in place). A stage is released to the UMMA
+// issuers by one tile-builder and one converter arrival.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+#include "spmm_sched.cuh"
 
 namespace dtc {
+namespace {
 
-dtc_status spmm_split_impl(const int32_t*, const uint8_t*, const int32_t*, const int32_t*,
-                           const float*, int32_t, int32_t, int64_t, int, const void*, const void*,
-                           int32_t, int, float*, int, int, float*, cudaStream_t) {
-  set_error("split-precision forms are not built yet");
-  return DTC_ERR_UNSUPPORTED;
+constexpr int kEpiWarps = 4;     // warps 0-3
+constexpr int kMmaWarp = 4;      // warps 4-5
+constexpr int kMmaWarps = 2;
+constexpr int kLoadWarp0 = kMmaWarp + kMmaWarps;   // warps 6-7
+constexpr int kLoadWarps = 2;
+constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;  // warps 8-11
+constexpr int kTileWarps = 4;
+constexpr int kConvWarp0 = kTileWarp0 + kTileWarps;  // warps 12-15
+constexpr int kConvWarps = 4;
+constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 512
+constexpr int kTileBytes = 4096;  // per block and 128-feature tile: 16 K rows x 128 bf16
+constexpr int kYBytes = 1024;     // 16 K x 32 N bf16, K-major core matrices
+
+enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2 };
+
+template <int FORM, int NT, int P, int S>
+struct SCfg {
+  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kMmaWarps == 0 &&
+                    S % kConvWarps == 0, "ownership");
+  static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
+  static constexpr int kNacc = (NT == 4) ? 2 : 4;
+  static constexpr int kStageX = P * NT * kTileBytes;
+  static constexpr int kRowStage = NT * 128;  // staged bytes of one gathered row (u8 / e4m3)
+  static constexpr int kStageE = (FORM == kFormBF16) ? 0 : P * kBlkW * kRowStage;
+  static constexpr int kStageY = P * kYBytes;
+  static constexpr int kX = S * kStageX;
+  static constexpr int kE = S * kStageE;
+  static constexpr int kY = S * kStageY;
+  static constexpr int kBars = (3 * S + 2 * kNacc) * 8;
+  static constexpr int kSmem = kX + kE + kY + kBars + 16 + 1024;
+  static constexpr int kCols = kMmaWarps * kNacc * NT * 32;
+  static_assert(kCols <= 512, "TMEM budget");
+  static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
+                                        : kCols <= 256 ? 256 : 512;
+};
+
+// Byte offset in one block tile of the 16-byte chunk j (features 8j..8j+7)
+// of K row k16 (0..7 hi, 8..15 lo): bf16 MN-major, 128-byte swizzle with
+// 16-byte granules; atoms of 64 features x 8 rows (LBO = 1024 B between the
+// two feature atoms, SBO = 2048 B between the hi and lo row groups).
+__device__ __forceinline__ uint32_t x_offset_bf16(uint32_t k16, uint32_t j) {
+  const uint32_t kk = k16 & 7;
+  return (k16 >> 3) * 2048 + (j >> 3) * 1024 + kk * 128 + (((j & 7) ^ kk) << 4);
+}
+
+// Byte offset of B-operand element (n, k): K-major, no swizzle, LBO = 128 B
+// between K halves, SBO = 256 B between 8-column groups.
+__device__ __forceinline__ uint32_t ysplit_offset(uint32_t n, uint32_t k) {
+  return (n & 7) * 16 + (n >> 3) * 256 + (k >> 3) * 128 + (k & 7) * 2;
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn(x));
+}
+
+template <int FORM, int NT, int P, int S, bool FOUR>
+__global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
+  using K = SCfg<FORM, NT, P, S>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint8_t* xring = smem;
+  uint8_t* ering = smem + K::kX;
+  uint8_t* yring = ering + K::kE;
+  uint64_t* bars = (uint64_t*)(yring + K::kY);
+  uint64_t* loaded = bars;               // [S] 32 cp.async arrivals
+  uint64_t* full = bars + S;             // [S] 1 tile-builder + 1 converter arrival
+  uint64_t* empty = bars + 2 * S;        // [S] UMMA commit
+  uint64_t* acc_full = bars + 3 * S;     // [kNacc] one commit per issuer
+  uint64_t* acc_empty = acc_full + K::kNacc;
+  uint32_t* tmem_slot = (uint32_t*)(acc_empty + K::kNacc);
+  volatile uint32_t* abort_flag = tmem_slot + 1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x;
+  const int col0 = blockIdx.y * NT * 128;
+  const int ncols = (p.N - col0) < NT * 128 ? (p.N - col0) : NT * 128;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&loaded[i], 32);
+      mbar_init(&full[i], 2);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < K::kNacc; ++i) {
+      mbar_init(&acc_full[i], kMmaWarps);
+      mbar_init(&acc_empty[i], kEpiWarps);
+    }
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (FORM != kFormSplit24) {  // lo rows stay zero for the single-plane forms
+    for (int i = threadIdx.x; i < S * P * NT; i += blockDim.x) {
+      float4* lo = reinterpret_cast<float4*>(xring + (size_t)i * kTileBytes + 2048);
+      for (int z = 0; z < 2048 / 16; ++z) lo[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    fence_proxy_async_smem();
+  }
+  if (warp == kMmaWarp) {
+    tmem_alloc(tmem_slot, K::kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  int64_t b0, b1;
+  cta_range(p, c, b0, b1);
+  const int64_t nblk = b1 - b0;
+  const int64_t nstage = (nblk + P - 1) / P;
+
+  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
+    // ------------------------------------------------------------ loaders
+    const int lw = warp - kLoadWarp0;
+    auto row_of = [&](int64_t st) -> int32_t {
+      const int64_t b = b0 + st * P + (lane >> 3);
+      return (lane < P * kBlkW && st < nstage && b < b1) ? __ldg(p.s2x + b * kBlkW + (lane & 7))
+                                                         : 0;
+    };
+    __shared__ int32_t rows_sm[kLoadWarps][32];  // SparseAToX of the stage being loaded
+    const uint8_t* plane0 = reinterpret_cast<const uint8_t*>(p.B);
+    const uint8_t* plane1 = reinterpret_cast<const uint8_t*>(p.B1);
+    int32_t rows = row_of(lw);
+    for (int64_t st = lw; st < nstage; st += kLoadWarps) {
+      const int s = (int)(st % S);
+      const uint32_t n = (uint32_t)(st / S);
+      const int32_t nxt = row_of(st + kLoadWarps);
+      const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
+      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      const int64_t sb = b0 + st * P;
+      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      const uint32_t xs = smem_u32(xring + (size_t)s * K::kStageX);
+      const uint32_t es = smem_u32(ering + (size_t)s * K::kStageE);
+      const uint8_t* eplane = FORM == kFormSplit24 ? plane1 : plane0;
+      if (ncols == NT * 128) {
+        // full 128-feature tiles: RPI gathered rows per warp instruction,
+        // CPR 16-byte chunks per row (compile-time)
+        for (int pb = 0; pb < nb; ++pb) {
+          if (FORM != kFormFP8) {  // bf16 hi plane -> K row k of the block tile, swizzled
+            constexpr int CPR = NT * 16, RPI = CPR >= 32 ? 1 : 32 / CPR;
+            constexpr int IPR = CPR >= 32 ? CPR / 32 : 1;
+#pragma unroll
+            for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
+              const int k = k0 + (RPI > 1 ? lane / CPR : 0);
+              const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+              const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
+              const uint8_t* src = plane0 + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
+#pragma unroll
+              for (int ii = 0; ii < IPR; ++ii) {
+                const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
+                cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(k, cc & 15),
+                           src + cc * 16, pad ? 0u : 16u);
+              }
+            }
+          }
+          if (FORM != kFormBF16) {  // u8 extension / e4m3 plane -> staging row
+            constexpr int CPR = NT * 8, RPI = CPR >= 32 ? 1 : 32 / CPR;
+            constexpr int IPR = CPR >= 32 ? CPR / 32 : 1;
+#pragma unroll
+            for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
+              const int k = k0 + (RPI > 1 ? lane / CPR : 0);
+              const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+              const bool pad = (k > 0 && r == 0);
+              const uint8_t* src = eplane + (int64_t)(pad ? 0 : r) * p.N + col0;
+#pragma unroll
+              for (int ii = 0; ii < IPR; ++ii) {
+                const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
+                cp_async16(es + (pb * kBlkW + k) * K::kRowStage + cc * 16, src + cc * 16,
+                           pad ? 0u : 16u);
+              }
+            }
+          }
+        }
+      } else {
+        // partial slice: lanes flattened over (gathered row, 16-byte chunk)
+        rows_sm[lw][lane] = rows;
+        __syncwarp();
+        const int nrow = nb * kBlkW;
+        if (FORM != kFormFP8) {
+          const int nck = ncols >> 3;
+          for (int idx = lane; idx < nrow * nck; idx += 32) {
+            const int rowi = idx / nck, cc = idx - rowi * nck;
+            const int k = rowi & 7, pb = rowi >> 3;
+            const int32_t r = rows_sm[lw][rowi];
+            const bool pad = (k > 0 && r == 0);
+            const uint8_t* src = plane0 + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
+            cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(k, cc & 15),
+                       src + cc * 16, pad ? 0u : 16u);
+          }
+        }
+        if (FORM != kFormBF16) {
+          const int nck = ncols >> 4;
+          for (int idx = lane; idx < nrow * nck; idx += 32) {
+            const int rowi = idx / nck, cc = idx - rowi * nck;
+            const int32_t r = rows_sm[lw][rowi];
+            const bool pad = ((rowi & 7) > 0 && r == 0);
+            const uint8_t* src = eplane + (int64_t)(pad ? 0 : r) * p.N + col0;
+            cp_async16(es + rowi * K::kRowStage + cc * 16, src + cc * 16, pad ? 0u : 16u);
+          }
+        }
+        __syncwarp();
+      }
+      cp_async_arrive_noinc(&loaded[s]);
+      rows = nxt;
+    }
+  } else if (warp >= kTileWarp0 && warp < kTileWarp0 + kTileWarps) {
+    // ------------------------------------------------------ tile builders
+    const int tw = warp - kTileWarp0;
+    auto offs_of = [&](int64_t st) -> int32_t {
+      const int64_t sb = b0 + st * P;
+      return (st < nstage && lane <= P && sb + lane <= b1) ? __ldg(p.toff + sb + lane) : 0;
+    };
+    int32_t offv = offs_of(tw);
+    for (int64_t st = tw; st < nstage; st += kTileWarps) {
+      const int s = (int)(st % S);
+      const uint32_t n = (uint32_t)(st / S);
+      const int32_t nxt = offs_of(st + kTileWarps);
+      const int64_t sb = b0 + st * P;
+      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      int32_t off[P + 1];
+#pragma unroll
+      for (int k = 0; k <= P; ++k) off[k] = __shfl_sync(0xffffffffu, offv, k);
+      const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
+      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      uint8_t* ys = yring + (size_t)s * K::kStageY;
+      for (int z = lane; z < P * kYBytes / 16; z += 32)
+        reinterpret_cast<float4*>(ys)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncwarp();
+      const int32_t e0 = off[0], e1 = off[nb];
+      for (int32_t e = e0 + lane; e < e1; e += 32) {
+        int pb = 0;
+#pragma unroll
+        for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
+        const uint32_t pos = __ldg(p.tile + e);
+        const float v = p.vals ? __ldg(p.vals + e) : 1.0f;
+        if (pos >= kWinH * kBlkW) {
+          atomicOr(p.err, kErrBadIndex);
+          continue;
+        }
+        if (v == 0.0f) continue;
+        const uint32_t r = pos >> 3, sl = pos & 7;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const uint16_t hb = __bfloat16_as_ushort(hi);
+        const uint16_t lb = bf16_bits(v - __bfloat162float(hi));
+        uint8_t* yb = ys + pb * kYBytes;
+        *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, sl)) = hb;
+        *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, 8 + sl)) = hb;
+        *reinterpret_cast<uint16_t*>(yb + ysplit_offset(16 + r, sl)) = lb;
+        if (FOUR) *reinterpret_cast<uint16_t*>(yb + ysplit_offset(16 + r, 8 + sl)) = lb;
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[s]);
+      offv = nxt;
+    }
+  } else if (warp >= kConvWarp0) {
+    // --------------------------------------------------------- converters
+    const int cw = warp - kConvWarp0;
+    __shared__ float row_scale[kConvWarps][32];  // FP8: scale of stage row (pb*8 + k)
+    auto scale_of = [&](int64_t st) -> float {
+      if (FORM != kFormFP8) return 1.0f;
+      const int64_t b = b0 + st * P + (lane >> 3);
+      if (!(lane < P * kBlkW && st < nstage && b < b1)) return 0.0f;
+      const int32_t r = __ldg(p.s2x + b * kBlkW + (lane & 7));
+      return ((lane & 7) > 0 && r == 0) ? 0.0f : __ldg(reinterpret_cast<const float*>(p.B1) + r);
+    };
+    float scv = scale_of(cw);
+    const int nchunk = ncols >> 3;  // 8-feature chunks per gathered row
+    for (int64_t st = cw; st < nstage; st += kConvWarps) {
+      const int s = (int)(st % S);
+      const uint32_t n = (uint32_t)(st / S);
+      const float scn = scale_of(st + kConvWarps);
+      const int64_t sb = b0 + st * P;
+      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      const bool got = mbar_wait(&loaded[s], n & 1, p.err);  // implies the stage was empty
+      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      if (FORM == kFormFP8) {
+        row_scale[cw][lane] = scv;
+        __syncwarp();
+      }
+      if (FORM != kFormBF16) {
+        uint8_t* xs = xring + (size_t)s * K::kStageX;
+        const uint8_t* es = ering + (size_t)s * K::kStageE;
+        const int items = nb * kBlkW * nchunk;
+        // item it: 8 features (16 B of bf16) of gathered row rowi = pb * 8 + k
+        auto locate = [&](int it, uint32_t& xoff, uint32_t& eoff, int& rowi) {
+          rowi = nchunk == NT * 16 ? it / (NT * 16) : it / nchunk;
+          const int j = it - rowi * nchunk;
+          xoff = (uint32_t)(((rowi >> 3) * NT + (j >> 4)) * kTileBytes) +
+                 x_offset_bf16(rowi & 7, j & 15);
+          eoff = (uint32_t)(rowi * K::kRowStage + j * 8);
+        };
+        // SPLIT24: lo = b24 - hi is exact in bf16, so its bf16 bits are the
+        // top half of the fp32 difference. Per element pair: the hi bits go
+        // to the top of two fp32 words (byte permutes), the extension bytes
+        // under them, one packed fp32x2 subtraction, one permute to pack.
+        auto lo_words = [&](const uint4& h, const uint2& e, uint32_t (&o)[4]) {
+          const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
+          const uint32_t ew[2] = {e.x, e.y};
+#pragma unroll
+          for (int z = 0; z < 4; ++z) {
+            const uint32_t eword = ew[z >> 1];
+            const uint32_t sel0 = 0x3200u | ((4u + 2u * (z & 1)) << 4);      // ext byte 2z
+            const uint32_t sel1 = 0x3200u | ((4u + 2u * (z & 1) + 1u) << 4); // ext byte 2z+1
+            const uint32_t h0 = __byte_perm(hw[z], 0u, 0x1044);
+            const uint32_t h1 = hw[z] & 0xFFFF0000u;
+            const uint32_t b0 = __byte_perm(h0, eword, sel0);
+            const uint32_t b1 = __byte_perm(h1, eword, sel1);
+            uint32_t l0, l1;
+            asm("{\n\t.reg .b64 a, b, d;\n\t"
+                "mov.b64 a, {%2, %3};\n\t"
+                "mov.b64 b, {%4, %5};\n\t"
+                "sub.rn.f32x2 d, a, b;\n\t"
+                "mov.b64 {%0, %1}, d;\n\t}"
+                : "=r"(l0), "=r"(l1)
+                : "r"(b0), "r"(b1), "r"(h0), "r"(h1));
+            o[z] = __byte_perm(l0, l1, 0x7632);
+          }
+        };
+        auto fp8_words = [&](const uint2& e, float sc, uint32_t (&o)[4]) {
+          const uint32_t ew[2] = {e.x, e.y};
+#pragma unroll
+          for (int z = 0; z < 4; ++z) {
+            const uint16_t q2 = (uint16_t)(ew[z >> 1] >> ((z & 1) * 16));
+            const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)q2, __NV_E4M3);
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&hr));
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(f.x * sc, f.y * sc);
+            o[z] = *reinterpret_cast<const uint32_t*>(&b2);
+          }
+        };
+        constexpr int U = 4;  // independent items per trip: all loads first, then math, then stores
+        int it = lane;
+        for (; it + 32 * (U - 1) < items; it += 32 * U) {
+          uint32_t xo[U], eo[U];
+          int ri[U];
+          uint4 h[U];
+          uint2 e[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            locate(it + 32 * u, xo[u], eo[u], ri[u]);
+            e[u] = *reinterpret_cast<const uint2*>(es + eo[u]);
+            if (FORM == kFormSplit24) h[u] = *reinterpret_cast<const uint4*>(xs + xo[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            uint32_t o[4];
+            if (FORM == kFormSplit24) {
+              lo_words(h[u], e[u], o);
+              *reinterpret_cast<uint4*>(xs + xo[u] + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
+            } else {
+              fp8_words(e[u], row_scale[cw][ri[u]], o);
+              *reinterpret_cast<uint4*>(xs + xo[u]) = make_uint4(o[0], o[1], o[2], o[3]);
+            }
+          }
+        }
+        for (; it < items; it += 32) {
+          uint32_t xo, eo;
+          int ri;
+          locate(it, xo, eo, ri);
+          const uint2 e = *reinterpret_cast<const uint2*>(es + eo);
+          uint32_t o[4];
+          if (FORM == kFormSplit24) {
+            lo_words(*reinterpret_cast<const uint4*>(xs + xo), e, o);
+            *reinterpret_cast<uint4*>(xs + xo + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
+          } else {
+            fp8_words(e, row_scale[cw][ri], o);
+            *reinterpret_cast<uint4*>(xs + xo) = make_uint4(o[0], o[1], o[2], o[3]);
+          }
+        }
+        fence_proxy_async_smem();
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[s]);
+      scv = scn;
+    }
+  } else if (warp >= kMmaWarp && warp < kMmaWarp + kMmaWarps) {
+    // ------------------------------------------------------------- UMMA
+    if (lane == 0) {
+      const int m = warp - kMmaWarp;
+      int32_t ws, we;
+      cta_windows(p, c, b0, b1, ws, we);
+      constexpr uint32_t idesc = umma_idesc(1, 128, 32, 1, 0);
+      const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 2048, 2);
+      const uint64_t bdesc0 = umma_desc(smem_u32(yring), 128, 256, 0);
+      uint32_t q = 0;
+      bool ok = true;
+      int64_t r0 = ws < we ? __ldg(p.rwo + ws) : 0;
+      int64_t r1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
+      for (int32_t w = ws; w < we && ok; ++w) {
+        const int64_t r2 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;
+        const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
+        r0 = r1;
+        r1 = r2;
+        if (s0 >= s1) continue;
+        const int a = (int)(q % K::kNacc);
+        if (!mbar_wait(&acc_empty[a], ((q / K::kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t dtm = tmem_base + (uint32_t)((m * K::kNacc + a) * NT * 32);
+        uint32_t acc = 0;
+        int64_t st = (s0 - b0) / P;
+        st += (m - (int)(st % kMmaWarps) + kMmaWarps) % kMmaWarps;
+        const int64_t st_last = (s1 - 1 - b0) / P;
+        for (; st <= st_last; st += kMmaWarps) {
+          const int s = (int)(st % S);
+          const int64_t sb = b0 + st * P;
+          const int64_t lo = sb > s0 ? sb : s0;
+          const int64_t hi = (sb + P) < s1 ? (sb + P) : s1;
+          if (lo == sb) {
+            if (!mbar_wait(&full[s], (uint32_t)(st / S) & 1, p.err)) { ok = false; break; }
+            fence_proxy_async_smem();
+            tc_fence_after();
+          }
+          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * kYBytes) >> 4);
+          uint64_t adesc =
+              adesc0 + (uint64_t)((s * K::kStageX + (int)(lo - sb) * NT * kTileBytes) >> 4);
+          for (int64_t b = lo; b < hi; ++b) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+              mma_f16(dtm + t * 32, adesc + (uint64_t)(t * (kTileBytes >> 4)), bdesc, idesc, acc);
+            acc = 1;
+            adesc += (uint64_t)((NT * kTileBytes) >> 4);
+            bdesc += (uint64_t)(kYBytes >> 4);
+          }
+          if (hi == sb + P || hi == b1) tc_commit(&empty[s]);
+        }
+        if (!ok) break;
+        tc_commit(&acc_full[a]);
+        ++q;
+      }
+      if (!ok) *abort_flag = 1;
+    }
+    __syncwarp();
+  } else {
+    // --------------------------------------------------------- epilogue
+    int32_t ws, we;
+    cta_windows(p, c, b0, b1, ws, we);
+    const int ew = warp;
+    uint32_t q = 0;
+    int64_t rn0 = ws < we ? __ldg(p.rwo + ws) : 0;
+    int64_t rn1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
+    for (int32_t w = ws; w < we; ++w) {
+      const int64_t r0 = rn0, r1 = rn1;
+      rn0 = rn1;
+      rn1 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;
+      const int64_t row0 = (int64_t)w * kWinH;
+      if (r0 == r1) {
+        for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
+          for (int r = 0; r < kWinH && row0 + r < p.M; ++r) p.C[(row0 + r) * p.N + f] = 0.0f;
+        continue;
+      }
+      const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
+      if (s0 >= s1) continue;
+      const int a = (int)(q % K::kNacc);
+      const bool got = mbar_wait(&acc_full[a], (q / K::kNacc) & 1, p.err);
+      if (!__all_sync(0xffffffffu, got)) { *abort_flag = 1; break; }
+      tc_fence_after();
+      float* out;
+      bool guard_rows = true;
+      if (p.mode == 1 && (r0 < b0 || r1 > b1)) {
+        const int slot = (r0 < b0) ? 2 * c : 2 * c + 1;
+        out = p.part + (size_t)slot * kWinH * p.N;
+        guard_rows = false;
+      } else {
+        out = p.C + row0 * p.N;
+      }
+      const int64_t st0 = (s0 - b0) / P, st1 = (s1 - 1 - b0) / P;
+      const bool both = st1 > st0;
+      const int m0 = (int)(st0 % kMmaWarps);
+      const uint32_t lane_addr = tmem_base + ((uint32_t)(ew * 32) << 16);
+#pragma unroll 1
+      for (int t = 0; t < NT; ++t) {
+        float x[16];
+#pragma unroll
+        for (int r = 0; r < kWinH; ++r) x[r] = 0.0f;
+        // fixed order: issuer 0's partial, then issuer 1's
+#pragma unroll 1
+        for (int mi = 0; mi < kMmaWarps; ++mi) {
+          if (!both && mi != m0) continue;
+          uint32_t v[16], u[16];
+          const uint32_t col = (uint32_t)(((mi * K::kNacc + a) * NT + t) * 32);
+          tmem_ld16(lane_addr + col, v);
+          tmem_ld16(lane_addr + col + 16, u);
+          tmem_ld_wait();
+#pragma unroll
+          for (int r = 0; r < kWinH; ++r) x[r] += __uint_as_float(v[r]) + __uint_as_float(u[r]);
+        }
+        const int f = col0 + t * 128 + ew * 32 + lane;
+        if (t == NT - 1) {
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[a]);
+        }
+        if (f < p.N) {
+#pragma unroll
+          for (int r = 0; r < kWinH; ++r)
+            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = x[r];
+        }
+      }
+      ++q;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, K::kTmemCols);
+  }
+}
+
+template <int FORM, int NT, int P, int S, bool FOUR>
+dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
+  constexpr int smem = SCfg<FORM, NT, P, S>::kSmem;
+  static_assert(smem <= 227 * 1024, "shared memory budget");
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    DTC_CUDA(cudaFuncSetAttribute(k_spmm_split<FORM, NT, P, S, FOUR>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set[dev & 63] = true;
+  }
+  dim3 grid((unsigned)p.G, (unsigned)slices);
+  k_spmm_split<FORM, NT, P, S, FOUR><<<grid, kThreads, smem, st>>>(p);
+  DTC_CUDA(cudaGetLastError());
+  if (p.mode == 1 && p.G > 1) {
+    k_reduce_partials<<<p.G - 1, 256, 0, st>>>(p);
+    DTC_CUDA(cudaGetLastError());
+  }
+  return DTC_OK;
+}
+
+template <int FORM, bool FOUR>
+dtc_status dispatch_n(const Params& p, cudaStream_t st) {
+  if (p.N <= 128) return launch_split<FORM, 1, 4, 8, FOUR>(p, 1, st);
+  if (p.N <= 256) return launch_split<FORM, 2, 2, 8, FOUR>(p, 1, st);
+  return launch_split<FORM, 4, 1, 8, FOUR>(p, (p.N + 511) / 512, st);
+}
+
+}  // namespace
+
+dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                           int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
+                           int precision, float* C, int mode, int grid, float* part,
+                           cudaStream_t st) {
+  DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
+  DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8,
+              "split kernels take SPLIT24, BF16 or FP8 B");
+  DTC_REQUIRE(precision == DTC_PREC_SPLIT3 || precision == DTC_PREC_SPLIT4,
+              "split kernels take precision SPLIT3 or SPLIT4");
+  DTC_REQUIRE(N % 16 == 0, "split forms need N % 16 == 0 (16-byte row segments of every plane)");
+  DTC_REQUIRE(bformat == DTC_B_BF16 || p1 != nullptr, "second B plane missing");
+  DTC_REQUIRE(((uintptr_t)p0 & 15) == 0 && ((uintptr_t)p1 & 15) == 0, "planes must be 16-byte aligned");
+  DTC_REQUIRE(nwin == (M + kWinH - 1) / kWinH, "num_windows must be ceil(num_nodes/16)");
+  DTC_REQUIRE(mode == 0 || part != nullptr, "balance mode needs the partials workspace");
+  if (!is_sm100()) {
+    set_error("tcgen05 kernels need an sm_100 device");
+    return DTC_ERR_UNSUPPORTED;
+  }
+  if (M == 0) return DTC_OK;
+  if (T == 0) {
+    DTC_CUDA(cudaMemsetAsync(C, 0, (size_t)M * N * sizeof(float), st));
+    return DTC_OK;
+  }
+  Params p{};
+  p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals;
+  p.B = reinterpret_cast<const float*>(p0); p.B1 = p1; p.bformat = bformat;
+  p.C = C; p.part = part; p.err = device_error_word();
+  p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
+  int G = grid > 0 ? grid : default_grid();
+  if ((int64_t)G > T) G = (int)T;
+  p.G = G;
+  const bool four = precision == DTC_PREC_SPLIT4;
+  switch (bformat) {
+    case DTC_B_SPLIT24:
+      return four ? dispatch_n<kFormSplit24, true>(p, st) : dispatch_n<kFormSplit24, false>(p, st);
+    case DTC_B_BF16:
+      return four ? dispatch_n<kFormBF16, true>(p, st) : dispatch_n<kFormBF16, false>(p, st);
+    default:
+      return four ? dispatch_n<kFormFP8, true>(p, st) : dispatch_n<kFormFP8, false>(p, st);
+  }
 }
 
 }  // namespace dtc

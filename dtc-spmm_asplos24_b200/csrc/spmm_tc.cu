@@ -37,7 +37,7 @@
 // ahead would pass spuriously). Every wait is bounded (2 s) and records
 // kErrWaitTimeout instead of hanging.
 #include <cuda_bf16.h>
-#include "common.cuh"
+#include "spmm_sched.cuh"
 
 namespace dtc {
 namespace {
@@ -51,68 +51,8 @@ constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;
 constexpr int kTileWarps = 4;
 constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 448
 constexpr int kNacc = 4;        // TMEM accumulator buffers in flight
-constexpr int kWinH = 16;       // row-window height (BLK_H)
-constexpr int kBlkW = 8;        // TC-block width (BLK_W)
 constexpr int kXTileBytes = 4096;   // 8 rows x 128 fp32 features
 constexpr int kYBytes = 512;        // 16 x 8 fp32, K-major core matrices
-
-struct Params {
-  const int32_t* rwo;        // RowWindowOffset [nwin+1]
-  const uint8_t* tile;       // TCblocktileId [nnz]
-  const int32_t* toff;       // TCblockoffset [T+1]
-  const int32_t* s2x;        // SparseAToX [T*8]
-  const float* vals;         // tile-order values or null (A = 1)
-  const float* B;            // [M x N] fp32
-  float* C;                  // [M x N]
-  float* part;               // partial tiles [2*G x 16 x N] (balance mode)
-  uint32_t* err;
-  int32_t M, nwin, N, G, mode;
-  int64_t T;
-};
-
-__device__ __forceinline__ int32_t lower_bound_i32(const int32_t* a, int32_t n, int64_t x) {
-  int32_t lo = 0, hi = n;
-  while (lo < hi) {
-    int32_t mid = (lo + hi) >> 1;
-    if ((int64_t)__ldg(a + mid) < x) lo = mid + 1; else hi = mid;
-  }
-  return lo;
-}
-
-// CTA block range (see header comment).
-__device__ __forceinline__ void cta_range(const Params& p, int c, int64_t& b0, int64_t& b1) {
-  b0 = (int64_t)c * p.T / p.G;
-  b1 = (int64_t)(c + 1) * p.T / p.G;
-  if (p.mode == 0) {  // snap to window starts: windows never split
-    int32_t w0 = lower_bound_i32(p.rwo, p.nwin, b0);
-    b0 = (w0 < p.nwin) ? __ldg(p.rwo + w0) : p.T;
-    if (c + 1 < p.G) {
-      int32_t w1 = lower_bound_i32(p.rwo, p.nwin, b1);
-      b1 = (w1 < p.nwin) ? __ldg(p.rwo + w1) : p.T;
-    } else {
-      b1 = p.T;
-    }
-  }
-}
-
-// Windows walked by a CTA: [w_start, w_end). Empty windows in the range are
-// owned by this CTA (their C rows are zeroed here); nonempty windows whose
-// intersection with [b0, b1) is empty are skipped.
-__device__ __forceinline__ void cta_windows(const Params& p, int c, int64_t b0, int64_t b1,
-                                            int32_t& w_start, int32_t& w_end) {
-  int32_t wl = lower_bound_i32(p.rwo, p.nwin, b0);
-  if (wl > 0 && (wl == p.nwin || (int64_t)__ldg(p.rwo + wl) > b0)) wl -= 1;
-  w_start = wl;
-  w_end = (c + 1 == p.G) ? p.nwin : lower_bound_i32(p.rwo, p.nwin, b1);
-}
-
-// Byte offset of A_b^T element (window row r, slot s) in the K-major,
-// no-swizzle core-matrix layout (8 rows x 16 B core matrices; LBO = 128 B
-// between the two K halves, SBO = 256 B between the two 8-row groups).
-__device__ __forceinline__ uint32_t y_offset(uint32_t pos) {
-  uint32_t r = pos >> 3, s = pos & 7;
-  return (r & 7) * 16 + (r >> 3) * 256 + (s >> 2) * 128 + (s & 3) * 4;
-}
 
 // Byte offset, inside one 8-row x 128-feature fp32 tile, of 16-byte chunk
 // `cc` (features 4cc..4cc+3) of row k, in the UMMA layout-type-1 atom order:
@@ -121,16 +61,6 @@ __device__ __forceinline__ uint32_t x_offset_tf32(uint32_t k, uint32_t cc) {
   const uint32_t a = cc >> 3, j = cc & 7;
   const uint32_t g = (j >> 1) ^ (k & 3);
   return a * 1024 + (k >> 2) * 512 + (k & 3) * 128 + ((g << 1) | (j & 1)) * 16;
-}
-
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
-               "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
 }
 
 template <int NT, int P, int S>
@@ -205,6 +135,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       return (lane < P * kBlkW && st < nstage && b < b1) ? __ldg(p.s2x + b * kBlkW + (lane & 7))
                                                          : 0;
     };
+    __shared__ int32_t rows_sm[kLoadWarps][32];  // SparseAToX of the stage being loaded
     int32_t rows = row_of(lw);
     for (int64_t st = lw; st < nstage; st += kLoadWarps) {
       const int s = (int)(st % S);
@@ -215,18 +146,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       const int64_t sb = b0 + st * P;
       const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
       const uint32_t xs = smem_u32(xring + (size_t)s * K::kStageX);
-      for (int pb = 0; pb < nb; ++pb) {
+      if (nck == NT * 32) {
+        // full 128-feature tiles: one gathered row per warp instruction
+        for (int pb = 0; pb < nb; ++pb) {
 #pragma unroll
-        for (int k = 0; k < kBlkW; ++k) {
-          const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
-          const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
-          const float* src = p.B + (int64_t)(pad ? 0 : r) * p.N + col0;
-          for (int cc = lane; cc < nck; cc += 32) {
-            const int t = cc >> 5;
-            cp_async16(xs + (pb * NT + t) * kXTileBytes + x_offset_tf32(k, cc & 31), src + cc * 4,
-                       pad ? 0u : 16u);
+          for (int k = 0; k < kBlkW; ++k) {
+            const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+            const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
+            const float* src = p.B + (int64_t)(pad ? 0 : r) * p.N + col0;
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+              cp_async16(xs + (pb * NT + t) * kXTileBytes + x_offset_tf32(k, lane),
+                         src + (t * 32 + lane) * 4, pad ? 0u : 16u);
           }
         }
+      } else {
+        // partial slice: lanes flattened over (gathered row, 16-byte chunk)
+        rows_sm[lw][lane] = rows;
+        __syncwarp();
+        for (int idx = lane; idx < nb * kBlkW * nck; idx += 32) {
+          const int rowi = idx / nck, cc = idx - rowi * nck;
+          const int k = rowi & 7, pb = rowi >> 3;
+          const int32_t r = rows_sm[lw][rowi];
+          const bool pad = (k > 0 && r == 0);
+          const float* src = p.B + (int64_t)(pad ? 0 : r) * p.N + col0;
+          cp_async16(xs + (pb * NT + (cc >> 5)) * kXTileBytes + x_offset_tf32(k, cc & 31),
+                     src + cc * 4, pad ? 0u : 16u);
+        }
+        __syncwarp();
       }
       cp_async_arrive_noinc(&full[s]);
       rows = nxt;
@@ -415,37 +362,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
   }
 }
 
-// Sums the partial tiles of every window cut by CTA boundaries, in CTA order
-// (bitwise reproducible), and writes its C rows. One CTA per boundary.
-__global__ void k_reduce_partials(const Params p) {
-  const int c = blockIdx.x + 1;  // boundary between CTA c-1 and c
-  const int64_t bc = (int64_t)c * p.T / p.G;
-  const int64_t bprev = (int64_t)(c - 1) * p.T / p.G;
-  // window containing block bc: largest w with rwo[w] <= bc
-  int32_t lo = 0, hi = p.nwin;
-  while (lo < hi) {
-    int32_t mid = (lo + hi + 1) >> 1;
-    if (__ldg(p.rwo + mid) <= bc) lo = mid; else hi = mid - 1;
-  }
-  const int32_t w = lo;
-  if (w >= p.nwin) return;
-  const int64_t r0 = __ldg(p.rwo + w), r1 = __ldg(p.rwo + w + 1);
-  if (!(r0 < bc && bc < r1)) return;           // boundary not inside window w
-  if (c - 1 >= 1 && bprev > r0) return;        // an earlier boundary owns it
-  // contributors: CTA c-1 (tail slot), CTAs c..c_last (head slots)
-  int c_last = c;
-  while (c_last + 1 < p.G && (int64_t)(c_last + 1) * p.T / p.G < r1) ++c_last;
-  const int64_t row0 = (int64_t)w * kWinH;
-  const int64_t elems = (int64_t)kWinH * p.N;
-  for (int64_t x = threadIdx.x; x < elems; x += blockDim.x) {
-    const int r = (int)(x / p.N);
-    if (row0 + r >= p.M) continue;
-    float acc = p.part[(size_t)(2 * (c - 1) + 1) * elems + x];
-    for (int k = c; k <= c_last; ++k) acc += p.part[(size_t)(2 * k) * elems + x];
-    p.C[row0 * p.N + x] = acc;
-  }
-}
-
 __global__ void k_rowid_to_rwo(const int32_t* __restrict__ rowid, int64_t T, int32_t nwin,
                                int32_t* __restrict__ rwo) {
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -502,7 +418,7 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
   p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals; p.B = B;
   p.C = C; p.part = part; p.err = device_error_word();
   p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
-  int G = grid > 0 ? grid : num_sms();
+  int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
   if (N <= 128) return launch_tf32<1, 4, 8>(p, 1, st);
@@ -511,7 +427,7 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
 }
 
 size_t spmm_partials_bytes(int64_t T, int32_t N, int grid) {
-  int G = grid > 0 ? grid : num_sms();
+  int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)(T > 0 ? T : 1);
   return (size_t)2 * G * kWinH * (size_t)N * sizeof(float);
 }

@@ -258,3 +258,76 @@ void oracle_metcf_spmm_f64(const int32_t* rowWindowOffset, const uint8_t* tileId
   }
   free(tile);
 }
+
+/* ---------------------------------------------------------------------------
+ * Dense-operand storage forms, restated from their definitions (the device
+ * packers live in the product's formats.cu; these are the checkers).
+ * ------------------------------------------------------------------------- */
+
+/* fp32 rounded to nearest-even at 16 significant bits, split into the bf16
+ * top half ("hi") and the next 8 mantissa bits ("ext"). NaN -> canonical
+ * quiet NaN, +-Inf kept. */
+void oracle_pack_split24(const float* B, int64_t n, uint16_t* hi, uint8_t* ext) {
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t u;
+    memcpy(&u, &B[i], 4);
+    uint32_t e = (u >> 23) & 0xFF;
+    uint32_t r;
+    if (e == 0xFF) r = (u & 0x7FFFFF) ? 0x7FC00000u : u;
+    else r = (u + 0x7Fu + ((u >> 8) & 1u)) & 0xFFFFFF00u;
+    hi[i] = (uint16_t)(r >> 16);
+    ext[i] = (uint8_t)(r >> 8);
+  }
+}
+
+/* fp32 -> bf16, round to nearest even; NaN -> quiet NaN keeping the sign. */
+void oracle_pack_bf16(const float* B, int64_t n, uint16_t* out) {
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t u;
+    memcpy(&u, &B[i], 4);
+    if (((u >> 23) & 0xFF) == 0xFF && (u & 0x7FFFFF)) { out[i] = (uint16_t)((u >> 16) | 0x40); continue; }
+    out[i] = (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+  }
+}
+
+/* fp32 -> e4m3 (1 sign, 4 exponent bits with bias 7, 3 mantissa bits; no
+ * infinities, S.1111.111 is NaN, largest finite 448), round to nearest even,
+ * saturating to +-448. */
+static uint8_t e4m3_rn_sat(float y) {
+  if (isnan(y)) return 0x7F;
+  uint8_t sign = signbit(y) ? 0x80 : 0x00;
+  double a = fabs((double)y);
+  if (a >= 448.0) return sign | 0x7E;
+  if (a < ldexp(1.0, -6)) {                 /* subnormal range: multiples of 2^-9 */
+    double m = nearbyint(a * 512.0);        /* 0..8; 8 encodes the smallest normal */
+    return sign | (uint8_t)m;
+  }
+  int e;
+  frexp(a, &e);                             /* a = f * 2^e, f in [0.5, 1) */
+  e -= 1;                                   /* a in [2^e, 2^(e+1)) */
+  double t = nearbyint(ldexp(a, 3 - e));    /* 8..16 */
+  if (t >= 16.0) { t = 8.0; e += 1; }
+  if (e > 8 || (e == 8 && t > 14.0)) return sign | 0x7E;
+  return sign | (uint8_t)(((e + 7) << 3) | ((int)t - 8));
+}
+
+/* Per-row scale s = max|B[r,:]| / 448 (1 when the row is all zero or not
+ * finite), q = e4m3(B / s). */
+void oracle_pack_fp8(const float* B, int64_t rows, int32_t N, uint8_t* q, float* scale) {
+  for (int64_t r = 0; r < rows; r++) {
+    const float* x = B + r * N;
+    float m = 0.0f;
+    for (int32_t j = 0; j < N; j++) { float v = fabsf(x[j]); if (v > m) m = v; }
+    float s = (m > 0.0f && isfinite(m)) ? m / 448.0f : 1.0f;
+    scale[r] = s;
+    for (int32_t j = 0; j < N; j++) q[r * N + j] = e4m3_rn_sat(x[j] / s);
+  }
+}
+
+/* Value of an e4m3 byte (for error bounds in tests). */
+float oracle_e4m3_value(uint8_t b) {
+  int s = b >> 7, e = (b >> 3) & 0xF, m = b & 7;
+  if (e == 0xF && m == 7) return NAN;
+  float v = e == 0 ? ldexpf((float)m, -9) : ldexpf(1.0f + m / 8.0f, e - 7);
+  return s ? -v : v;
+}

@@ -128,3 +128,44 @@ def metcf_spmm_f64(m, M, B, H=16, W=8, tc_values=None):
                                 ctypes.c_int32(H), ctypes.c_int32(W), ctypes.c_int32(N),
                                 _p(B), _p(C))
     return C
+
+
+def pack_split24(B):
+    """fp32 -> (bf16 hi plane, u8 extension plane), RNE at 16 significant bits."""
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    hi = np.empty(B.shape, np.uint16)
+    ext = np.empty(B.shape, np.uint8)
+    lib().oracle_pack_split24(_p(B), ctypes.c_int64(B.size), _p(hi), _p(ext))
+    return hi, ext
+
+
+def pack_bf16(B):
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    out = np.empty(B.shape, np.uint16)
+    lib().oracle_pack_bf16(_p(B), ctypes.c_int64(B.size), _p(out))
+    return out
+
+
+def pack_fp8(B):
+    """fp32 rows -> (e4m3 bytes, fp32 per-row scales)."""
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    rows, N = B.shape
+    q = np.empty(B.shape, np.uint8)
+    s = np.empty(rows, np.float32)
+    lib().oracle_pack_fp8(_p(B), ctypes.c_int64(rows), ctypes.c_int32(N), _p(q), _p(s))
+    return q, s
+
+
+def e4m3_values(q):
+    """float32 values of an array of e4m3 bytes."""
+    L = lib()
+    L.oracle_e4m3_value.restype = ctypes.c_float
+    L.oracle_e4m3_value.argtypes = [ctypes.c_uint8]
+    table = np.array([L.oracle_e4m3_value(i) for i in range(256)], np.float32)
+    return table[q]
+
+
+def split24_values(hi, ext):
+    """fp32 values of the 24-bit form (the B the split kernels multiply)."""
+    u = (hi.astype(np.uint32) << 16) | (ext.astype(np.uint32) << 8)
+    return u.view(np.float32)
