@@ -38,8 +38,11 @@ SIGNATURES = {
     "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, C.c_int, C.c_int, szp],
     "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
     "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
+    "dtc_spmm_balance_noalloc": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp],
+    "dtc_noalloc_scratch_capacity": [],
 }
-_RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int}
+_RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int,
+             "dtc_noalloc_scratch_capacity": C.c_size_t}
 
 B_F32, B_SPLIT24, B_BF16, B_FP8 = 0, 1, 2, 3
 PREC_TF32, PREC_SPLIT3, PREC_SPLIT4 = 0, 1, 2

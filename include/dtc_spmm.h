@@ -134,6 +134,27 @@ dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tile
                             const float* d_B, int32_t N, float* d_C, void* d_workspace,
                             size_t workspace_bytes, dtc_stream_t stream);
 
+/* Strict-balance SpMM that allocates nothing and takes no workspace; no
+ * counterpart in the reference. For callers that cannot call cudaMalloc
+ * (inside a CUDA-graph capture, in a memory-budgeted server, in plugins or
+ * plain-C hosts without a device allocator): the window-offset table and the
+ * partial tiles live in a fixed 16 MiB array compiled into the library, held
+ * in the memory of every GPU that loads it until the process exits.
+ * Limit: 4*(ceil(num_nodes/16)+1) bytes (rounded up to 256) + 128*N bytes per
+ * SM (one CTA per SM) must fit in dtc_noalloc_scratch_capacity() bytes; larger
+ * problems get DTC_ERR_WORKSPACE_TOO_SMALL. The first call on a device looks
+ * up the array's device address with that device current -- make it before
+ * any stream capture. All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. Same results semantics as
+ * dtc_spmm_balance (deterministic for a given device). */
+dtc_status dtc_spmm_balance_noalloc(const int32_t* d_tcblockRowid, const uint8_t* d_tileId,
+                                    const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                                    const float* d_tcValues, int32_t num_nodes,
+                                    int64_t num_blocks, const float* d_B, int32_t N, float* d_C,
+                                    dtc_stream_t stream);
+/* Bytes of the built-in scratch array used by dtc_spmm_balance_noalloc. */
+size_t dtc_noalloc_scratch_capacity(void);
+
 /* General form used by the tuned paths: any B format / precision, explicit
  * schedule. mode 0 = window-scheduled, 1 = strict balance. grid = CTAs (0 =
  * one per SM). d_rowWindowOffset is required (build it from TCblockRowid with
