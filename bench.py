@@ -198,13 +198,62 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args):
+    """Batched uneven matrices: one graph-captured launch over the stacked batch
+    vs one window-scheduled launch per matrix (the reference-style loop)."""
+    import torch
+    from dtc_b200 import batched
+    torch.cuda.set_device(0)
+    N = args.N or 64
+    t0 = time.perf_counter()
+    mats, Bs = batched.zipf_batch(count=args.batch, N=N, seed=0)
+    gen_s = time.perf_counter() - t0
+    nnz = sum(m.nnz for m in mats)
+    flops = 2.0 * nnz * N
+    Bt = [torch.from_numpy(b).cuda() for b in Bs]
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    bs = batched.BatchedSpMM(mats, N)
+    bs.load(Bt)
+    bs.capture()
+    one_ms = timed(bs.run, args.steps, args.warmup)
+    ms_sep, run_sep = batched.separate_launches(mats, N)
+    outs = [torch.empty((m.M, N), device="cuda") for m in mats]
+    sep_ms = timed(lambda: run_sep(Bt, outs), max(3, args.steps // 4), 2)
+    line = {"metric": "batched SpMM GFLOP/s (2*nnz*N), one graph launch vs per-matrix launches",
+            "value": flops / (one_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": one_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "tf32",
+            "data": "synthetic",
+            "config": {"workload": f"{args.batch} zipf(2.1) matrices, rows log-uniform "
+                                   f"[256, 65536], N={N}", "nnz": int(nnz),
+                       "rows": int(sum(m.M for m in mats)), "T": bs.m.T},
+            "separate_launches_ms": sep_ms,
+            "separate_launches_gflops": flops / (sep_ms * 1e-3) / 1e9,
+            "speedup_vs_separate": sep_ms / one_ms, "gpu_launches": 2 * args.steps,
+            "generation_s": gen_s}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="rmat", choices=["rmat", "stencil", "uniform"])
+    ap.add_argument("--config", default="rmat", choices=["rmat", "stencil", "uniform", "batched"])
+    ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--scale", type=int, default=20)
     ap.add_argument("--N", type=int, default=0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -215,6 +264,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.config == "batched":
+        return run_batched(args)
 
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))

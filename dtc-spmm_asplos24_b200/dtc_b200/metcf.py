@@ -139,6 +139,15 @@ def pack_b(B: torch.Tensor, fmt: int):
     return [p0] if p1 is None else [p0, p1]
 
 
+def pack_b_into(B: torch.Tensor, fmt: int, planes):
+    """Re-pack B into existing planes (no allocation; usable inside graph capture)."""
+    B = B.contiguous()
+    rows, N = B.shape
+    call("dtc_pack_b", fmt, _ptr(B), rows, N, _ptr(planes[0]),
+         _ptr(planes[1]) if len(planes) > 1 else None, _stream())
+    return planes
+
+
 def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True, out=None,
             workspace=None):
     dev = planes[0].device
