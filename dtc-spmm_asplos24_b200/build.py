@@ -24,7 +24,8 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX")
 
 CU_SOURCES = ["abi.cu", "convert.cu", "spmm_tc.cu", "spmm_split.cu", "spmm_mma.cu", "formats.cu",
-              "noalloc.cu"]
+              "noalloc.cu", "tune.cu",
+              "relabel.cu"]
 GEN_SOURCES = ["gen.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", f"-I{INC}", f"-I{CSRC}"]

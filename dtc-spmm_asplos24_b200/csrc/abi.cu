@@ -9,12 +9,12 @@ namespace dtc {
 dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st);
+                          float* part, cudaStream_t st, int ntile = 0);
 dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st);
+                           cudaStream_t st, int ntile = 0);
 size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
 dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
                         cudaStream_t st);
@@ -180,10 +180,11 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
                        int64_t num_blocks, int bformat, const void* d_Bplane0,
                        const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
-                       int grid, void* d_workspace, size_t workspace_bytes,
+                       int grid, int ntile, void* d_workspace, size_t workspace_bytes,
                        dtc_stream_t stream) {
   DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
   DTC_REQUIRE(grid >= 0, "grid must be >= 0");
+  DTC_REQUIRE(ntile == 0 || ntile == 1 || ntile == 2 || ntile == 4, "ntile must be 0, 1, 2 or 4");
   DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_Bplane0 && d_C, "null device pointer");
   size_t need = 0;
   dtc_status s = dtc_spmm_ex_workspace_bytes(num_nodes, num_blocks, N, mode, grid, &need);
@@ -196,10 +197,11 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
   if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
     return spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
                           d_tcValues, num_nodes, num_windows, num_blocks,
-                          (const float*)d_Bplane0, N, d_C, mode, grid, (float*)d_workspace, st);
+                          (const float*)d_Bplane0, N, d_C, mode, grid, (float*)d_workspace, st,
+                          ntile);
   return spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
                          num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
-                         precision, d_C, mode, grid, (float*)d_workspace, st);
+                         precision, d_C, mode, grid, (float*)d_workspace, st, ntile);
 }
 
 dtc_status dtc_spmm_mma_sync(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,

@@ -186,7 +186,7 @@ std::vector<torch::Tensor> run_DTCSpMM_ex(std::vector<torch::Tensor> Bplanes, in
                                           torch::Tensor TCblocktileId, torch::Tensor TCblockoffset,
                                           torch::Tensor SparseAToX, int64_t num_nodes,
                                           int64_t precision, int64_t mode, int64_t grid,
-                                          c10::optional<torch::Tensor> values) {
+                                          c10::optional<torch::Tensor> values, int64_t ntile) {
   TORCH_CHECK(!Bplanes.empty(), "Bplanes is empty");
   for (auto& t : Bplanes) { CHECK_INPUT(t); }
   const c10::cuda::CUDAGuard guard(Bplanes[0].device());
@@ -202,8 +202,8 @@ std::vector<torch::Tensor> run_DTCSpMM_ex(std::vector<torch::Tensor> Bplanes, in
                     values_ptr(values, TCblocktileId.numel()), (int32_t)num_nodes, nwin, T,
                     (int)bformat, Bplanes[0].data_ptr(),
                     Bplanes.size() > 1 ? Bplanes[1].data_ptr() : nullptr, (int32_t)N,
-                    (int)precision, C.data_ptr<float>(), (int)mode, (int)grid, ws.data_ptr(), wsb,
-                    cur_stream()), "dtc_spmm_ex");
+                    (int)precision, C.data_ptr<float>(), (int)mode, (int)grid, (int)ntile,
+                    ws.data_ptr(), wsb, cur_stream()), "dtc_spmm_ex");
   return {C};
 }
 
@@ -252,7 +252,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("Bplanes"), py::arg("bformat"), py::arg("N"), py::arg("RowWindowOffset"),
         py::arg("TCblocktileId"), py::arg("TCblockoffset"), py::arg("SparseAToX"),
         py::arg("num_nodes"), py::arg("precision"), py::arg("mode") = 0, py::arg("grid") = 0,
-        py::arg("values") = py::none());
+        py::arg("values") = py::none(), py::arg("ntile") = 0);
   m.def("pack_b", &pack_b, "convert fp32 B into a storage form", py::arg("B"),
         py::arg("bformat"));
 }

@@ -568,9 +568,11 @@ dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
 }
 
 template <int FORM, bool FOUR>
-dtc_status dispatch_n(const Params& p, cudaStream_t st) {
-  if (p.N <= 128) return launch_split<FORM, 1, 4, 8, FOUR>(p, 1, st);
-  if (p.N <= 256) return launch_split<FORM, 2, 2, 8, FOUR>(p, 1, st);
+dtc_status dispatch_n(const Params& p, cudaStream_t st, int ntile) {
+  int nt = p.N <= 128 ? 1 : p.N <= 256 ? 2 : 4;
+  if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
+  if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR>(p, (p.N + 127) / 128, st);
+  if (nt == 2) return launch_split<FORM, 2, 2, 8, FOUR>(p, (p.N + 255) / 256, st);
   return launch_split<FORM, 4, 1, 8, FOUR>(p, (p.N + 511) / 512, st);
 }
 
@@ -580,7 +582,7 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st) {
+                           cudaStream_t st, int ntile) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8,
               "split kernels take SPLIT24, BF16 or FP8 B");
@@ -611,11 +613,11 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   const bool four = precision == DTC_PREC_SPLIT4;
   switch (bformat) {
     case DTC_B_SPLIT24:
-      return four ? dispatch_n<kFormSplit24, true>(p, st) : dispatch_n<kFormSplit24, false>(p, st);
+      return four ? dispatch_n<kFormSplit24, true>(p, st, ntile) : dispatch_n<kFormSplit24, false>(p, st, ntile);
     case DTC_B_BF16:
-      return four ? dispatch_n<kFormBF16, true>(p, st) : dispatch_n<kFormBF16, false>(p, st);
+      return four ? dispatch_n<kFormBF16, true>(p, st, ntile) : dispatch_n<kFormBF16, false>(p, st, ntile);
     default:
-      return four ? dispatch_n<kFormFP8, true>(p, st) : dispatch_n<kFormFP8, false>(p, st);
+      return four ? dispatch_n<kFormFP8, true>(p, st, ntile) : dispatch_n<kFormFP8, false>(p, st, ntile);
   }
 }
 

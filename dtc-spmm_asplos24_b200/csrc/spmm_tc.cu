@@ -400,7 +400,7 @@ dtc_status launch_tf32(const Params& p, int slices, cudaStream_t st) {
 dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st) {
+                          float* part, cudaStream_t st, int ntile) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0 (16-byte row segments)");
   DTC_REQUIRE(((uintptr_t)B & 15) == 0, "B must be 16-byte aligned");
@@ -421,8 +421,12 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
-  if (N <= 128) return launch_tf32<1, 4, 8>(p, 1, st);
-  if (N <= 256) return launch_tf32<2, 2, 8>(p, 1, st);
+  // N-tiles (128 features each) per CTA: all of N up to 4 tiles unless capped
+  // by `ntile`; wider slices of N go to more CTAs (grid.y).
+  int nt = N <= 128 ? 1 : N <= 256 ? 2 : 4;
+  if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
+  if (nt == 1) return launch_tf32<1, 4, 8>(p, (N + 127) / 128, st);
+  if (nt == 2) return launch_tf32<2, 2, 8>(p, (N + 255) / 256, st);
   return launch_tf32<4, 1, 8>(p, (N + 511) / 512, st);
 }
 

@@ -1,0 +1,159 @@
+// Exhaustive schedule autotuner for the TC-block SpMM (dtc_autotune).
+//
+// The reference picks its schedule from a hand-written table per dataset and
+// N (scripts/DTCSpMM/run_DTC_SpMM.py:10-30: balance or not, vector width,
+// N split). Here the schedule knobs of the tcgen05 kernels are measured
+// instead, on the caller's own ME-TCF arrays and B:
+//   mode   0 = window-scheduled (windows never split), 1 = strict balance
+//          (windows longer than the per-CTA chunk are split; the chunk,
+//          ceil(T / grid) blocks, is the split threshold)
+//   waves  CTAs = waves x SMs (one resident CTA per SM; more waves = smaller
+//          ranges, which evens out skew at the price of more range setup)
+//   ntile  128-feature tiles per CTA (fewer tiles spread wide N over more CTAs)
+// Each candidate runs once untimed and `reps` times between CUDA events on the
+// caller's stream; the mean is its time. Candidates change neither the B form
+// nor the product precision, only how fp32 partial sums are grouped; each
+// candidate's result is bitwise reproducible (window mode writes every C
+// element once, balance mode reduces its partial tiles in fixed order).
+#include <vector>
+#include "common.cuh"
+
+namespace dtc {
+dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                          const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                          int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
+                          float* part, cudaStream_t st, int ntile);
+dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
+                           int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
+                           int precision, float* C, int mode, int grid, float* part,
+                           cudaStream_t st, int ntile);
+size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
+}  // namespace dtc
+
+using namespace dtc;
+
+namespace {
+
+constexpr int kWaveChoices[] = {1, 2, 4, 8, 16};
+constexpr int kMaxWaves = 16;
+
+int auto_ntile(int32_t N) { return N <= 128 ? 1 : N <= 256 ? 2 : 4; }
+
+// Every distinct (mode, waves, ntile) the kernels support for this N.
+int candidates(int32_t N, dtc_schedule* out, int max) {
+  int n = 0;
+  const int nt_auto = auto_ntile(N);
+  for (int mode = 0; mode <= 1; ++mode)
+    for (int w : kWaveChoices)
+      for (int nt = 1; nt <= 4; nt *= 2) {
+        if (nt > nt_auto) break;
+        if (out && n < max) {
+          dtc_schedule& s = out[n];
+          s.mode = mode;
+          s.waves = w;
+          s.ntile = nt;
+          s.grid = 0;
+          s.ms = 0.0f;
+        }
+        ++n;
+      }
+  return n;
+}
+
+struct Events {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~Events() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int dtc_schedule_candidates(int32_t N, dtc_schedule* out, int max_out) {
+  if (N < 1) return 0;
+  return candidates(N, out, max_out);
+}
+
+dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                        size_t* bytes) {
+  DTC_REQUIRE(bytes != nullptr, "bytes is null");
+  DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
+  *bytes = spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms());
+  return DTC_OK;
+}
+
+dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                        int64_t num_blocks, int bformat, const void* d_Bplane0,
+                        const void* d_Bplane1, int32_t N, int precision, float* d_C,
+                        void* d_workspace, size_t workspace_bytes, int reps,
+                        dtc_schedule* results, int max_results, int* num_results, int* best,
+                        dtc_stream_t stream) {
+  DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_Bplane0 && d_C, "null device pointer");
+  DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
+  DTC_REQUIRE(reps >= 1 && reps <= 1000, "reps must be in [1, 1000]");
+  DTC_REQUIRE(best != nullptr, "best is null");
+  size_t need = 0;
+  dtc_status s = dtc_autotune_workspace_bytes(num_nodes, num_blocks, N, &need);
+  if (s != DTC_OK) return s;
+  if (!d_workspace || workspace_bytes < need) {
+    set_error("autotune workspace too small (dtc_autotune_workspace_bytes)");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  const bool tf32 = (bformat == DTC_B_F32 && precision == DTC_PREC_TF32);
+  if (tf32) {
+    DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0");
+  } else {
+    DTC_REQUIRE(N % 16 == 0, "split-precision path needs N % 16 == 0");
+  }
+  const int ncand = candidates(N, nullptr, 0);
+  std::vector<dtc_schedule> cand(ncand);
+  candidates(N, cand.data(), ncand);
+  cudaStream_t st = (cudaStream_t)stream;
+  Events ev;
+  DTC_CUDA(cudaEventCreate(&ev.a));
+  DTC_CUDA(cudaEventCreate(&ev.b));
+  const int sms = num_sms();
+  int best_i = -1;
+  for (int i = 0; i < ncand; ++i) {
+    dtc_schedule& c = cand[i];
+    int64_t g = (int64_t)c.waves * sms;
+    if (g > num_blocks) g = num_blocks > 0 ? num_blocks : 1;
+    c.grid = (int32_t)g;
+    auto run = [&]() {
+      return tf32 ? spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
+                                   d_tcValues, num_nodes, num_windows, num_blocks,
+                                   (const float*)d_Bplane0, N, d_C, c.mode, c.grid,
+                                   (float*)d_workspace, st, c.ntile)
+                  : spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
+                                    d_tcValues, num_nodes, num_windows, num_blocks, bformat,
+                                    d_Bplane0, d_Bplane1, N, precision, d_C, c.mode, c.grid,
+                                    (float*)d_workspace, st, c.ntile);
+    };
+    s = run();  // warm-up
+    if (s != DTC_OK) return s;
+    DTC_CUDA(cudaEventRecord(ev.a, st));
+    for (int r = 0; r < reps; ++r) {
+      s = run();
+      if (s != DTC_OK) return s;
+    }
+    DTC_CUDA(cudaEventRecord(ev.b, st));
+    DTC_CUDA(cudaEventSynchronize(ev.b));
+    float ms = 0.0f;
+    DTC_CUDA(cudaEventElapsedTime(&ms, ev.a, ev.b));
+    c.ms = ms / reps;
+    if (best_i < 0 || c.ms < cand[best_i].ms) best_i = i;
+  }
+  if (results)
+    for (int i = 0; i < ncand && i < max_results; ++i) results[i] = cand[i];
+  if (num_results) *num_results = ncand;
+  *best = best_i;
+  return DTC_OK;
+}
+
+}  // extern "C"

@@ -34,15 +34,35 @@ SIGNATURES = {
     "dtc_spmm_balance_workspace_bytes": [i32, i64, i32, szp],
     "dtc_spmm_balance": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp, sz, vp],
     "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
-                    C.c_int, C.c_int, vp, sz, vp],
+                    C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, C.c_int, C.c_int, szp],
     "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
     "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
     "dtc_spmm_balance_noalloc": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp],
     "dtc_noalloc_scratch_capacity": [],
+    "dtc_schedule_candidates": [i32, vp, C.c_int],
+    "dtc_relabel_workspace_bytes": [i32, i32, i64, szp],
+    "dtc_permute_csr": [vp, vp, vp, i32, i64, vp, vp, vp, vp, i64p, vp, sz, vp],
+    "dtc_transpose_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
+    "dtc_autotune_workspace_bytes": [i32, i64, i32, szp],
+    "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp, vp, sz,
+                     C.c_int, vp, C.c_int, vp, vp, vp],
 }
 _RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int,
-             "dtc_noalloc_scratch_capacity": C.c_size_t}
+             "dtc_noalloc_scratch_capacity": C.c_size_t, "dtc_schedule_candidates": C.c_int}
+
+
+class Schedule(C.Structure):
+    """dtc_schedule (include/dtc_spmm.h)."""
+    _fields_ = [("mode", C.c_int32), ("waves", C.c_int32), ("ntile", C.c_int32),
+                ("grid", C.c_int32), ("ms", C.c_float)]
+
+    def key(self):
+        return (self.mode, self.waves, self.ntile)
+
+    def __repr__(self):
+        return (f"Schedule(mode={self.mode}, waves={self.waves}, ntile={self.ntile}, "
+                f"grid={self.grid}, ms={self.ms:.4f})")
 
 B_F32, B_SPLIT24, B_BF16, B_FP8 = 0, 1, 2, 3
 PREC_TF32, PREC_SPLIT3, PREC_SPLIT4 = 0, 1, 2

@@ -149,7 +149,7 @@ def pack_b_into(B: torch.Tensor, fmt: int, planes):
 
 
 def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True, out=None,
-            workspace=None):
+            workspace=None, ntile=0):
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     wsb = C.c_size_t()
@@ -161,8 +161,48 @@ def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True
     call("dtc_spmm_ex", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId), _ptr(m.TCblockoffset),
          _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, fmt, _ptr(planes[0]),
          _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(C_), mode, grid,
-         _ptr(ws), 0 if ws is None else ws.numel(), _stream())
+         ntile, _ptr(ws), 0 if ws is None else ws.numel(), _stream())
     return C_
+
+
+def _relabel(name, rowptr, col, val, rows_out, extra):
+    dev = rowptr.device
+    rows_in = rowptr.numel() - 1
+    nnz = col.numel()
+    b = C.c_size_t()
+    K = extra[0] if name == "dtc_transpose_csr" else rows_in
+    call("dtc_relabel_workspace_bytes", rows_in, K, nnz, C.byref(b))
+    ws = torch.empty(max(b.value, 1), dtype=torch.uint8, device=dev)
+    rp = torch.empty(rows_out + 1, dtype=torch.int32, device=dev)
+    co = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+    vo = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev)
+    n = C.c_int64()
+    if name == "dtc_permute_csr":
+        call(name, _ptr(rowptr), _ptr(col), _ptr(val), rows_in, nnz, _ptr(extra[1]), _ptr(rp),
+             _ptr(co), _ptr(vo), C.byref(n), _ptr(ws), ws.numel(), _stream())
+    else:
+        call(name, _ptr(rowptr), _ptr(col), _ptr(val), rows_in, K, nnz, _ptr(rp), _ptr(co),
+             _ptr(vo), C.byref(n), _ptr(ws), ws.numel(), _stream())
+    return rp, co[: n.value], vo[: n.value]
+
+
+def permute_csr(rowptr, col, val, perm):
+    """P A Pᵀ (perm[new] = old) as canonical CSR: (rowptr, col, val) device tensors.
+
+    The GPU form of reordering/TCA_reorder.py:308-326 + the scipy CSR rebuild of
+    scripts/DTCSpMM/dataset.py:38-44 (columns sorted, duplicates summed).
+    """
+    i32 = lambda t: t.to(torch.int32).contiguous()
+    val = None if val is None else val.to(torch.float32).contiguous()
+    return _relabel("dtc_permute_csr", i32(rowptr), i32(col), val, rowptr.numel() - 1,
+                    (None, i32(perm)))
+
+
+def transpose_csr(rowptr, col, val, num_cols):
+    """Aᵀ as canonical CSR (num_cols rows): the operand of the backward product Aᵀ·G."""
+    i32 = lambda t: t.to(torch.int32).contiguous()
+    val = None if val is None else val.to(torch.float32).contiguous()
+    return _relabel("dtc_transpose_csr", i32(rowptr), i32(col), val, num_cols, (num_cols,))
 
 
 def device_status(clear=True):

@@ -80,6 +80,37 @@ dtc_status dtc_convert_fill(const int32_t* d_col, const int32_t* d_rowptr, int32
                             void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
+/* CSR relabelling. Output is canonical CSR: columns sorted within each row,  */
+/* duplicate (row, col) entries merged by summing their values in input CSR  */
+/* order (d_val == NULL counts each entry as 1, the reference's A = 1), the   */
+/* number of output entries stored in *nnz_out (synchronises `stream`).       */
+/* ------------------------------------------------------------------------- */
+dtc_status dtc_relabel_workspace_bytes(int32_t num_rows, int32_t num_cols, int64_t nnz,
+                                       size_t* bytes);
+
+/* Symmetric permutation P A Pᵀ of a square matrix: output row i is input row
+ * d_perm[i] with every column c renamed to the position of c in d_perm
+ * (d_perm[new] = old, a permutation of [0, num_nodes)). Replaces the
+ * reorder application of reordering/TCA_reorder.py:308-326 followed by the
+ * CSR rebuild of scripts/DTCSpMM/dataset.py:38-44 (scipy coo -> csr).
+ * d_val_out may be NULL. Output arrays hold num_nodes+1 / nnz entries. */
+dtc_status dtc_permute_csr(const int32_t* d_rowptr, const int32_t* d_col, const float* d_val,
+                           int32_t num_nodes, int64_t nnz, const int32_t* d_perm,
+                           int32_t* d_rowptr_out, int32_t* d_col_out, float* d_val_out,
+                           int64_t* nnz_out, void* d_workspace, size_t workspace_bytes,
+                           dtc_stream_t stream);
+
+/* Transpose: the num_cols x num_rows matrix Aᵀ, the operand of the backward
+ * product Aᵀ·G. The reference has no transpose: its backward entry points
+ * (DTC-SpMM/DTCSpMM.cpp:385-398) rerun the forward, valid only for symmetric
+ * A. Output arrays hold num_cols+1 / nnz entries. */
+dtc_status dtc_transpose_csr(const int32_t* d_rowptr, const int32_t* d_col, const float* d_val,
+                             int32_t num_rows, int32_t num_cols, int64_t nnz,
+                             int32_t* d_rowptr_out, int32_t* d_col_out, float* d_val_out,
+                             int64_t* nnz_out, void* d_workspace, size_t workspace_bytes,
+                             dtc_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
 /* Dense-operand storage forms ("B formats").                                  */
 /* ------------------------------------------------------------------------- */
 typedef enum {
@@ -157,16 +188,55 @@ size_t dtc_noalloc_scratch_capacity(void);
 
 /* General form used by the tuned paths: any B format / precision, explicit
  * schedule. mode 0 = window-scheduled, 1 = strict balance. grid = CTAs (0 =
- * one per SM). d_rowWindowOffset is required (build it from TCblockRowid with
- * dtc_rowid_to_window_offset). Workspace needed only for mode 1. */
+ * 16 per SM, run as waves). ntile = 128-feature tiles per CTA (0 = all of N
+ * up to 4; 1 or 2 split wider N across more CTAs). d_rowWindowOffset is
+ * required (build it from TCblockRowid with dtc_rowid_to_window_offset).
+ * Workspace needed only for mode 1. */
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
                        int64_t num_blocks, int bformat, const void* d_Bplane0,
                        const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
-                       int grid, void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+                       int grid, int ntile, void* d_workspace, size_t workspace_bytes,
+                       dtc_stream_t stream);
 dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
                                        int grid, size_t* bytes);
+
+/* ------------------------------------------------------------------------- */
+/* Schedule autotuner. Replaces the reference's hand-written schedule table   */
+/* (scripts/DTCSpMM/run_DTC_SpMM.py:10-30: balance yes/no, vector width and   */
+/* N split chosen per dataset and N) by measurement on the caller's data.     */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  int32_t mode;   /* 0 = window-scheduled (no window split), 1 = strict balance */
+  int32_t waves;  /* CTAs = waves x SMs, capped at T; in mode 1 the split       */
+                  /* threshold is ceil(T / CTAs) TC blocks per CTA             */
+  int32_t ntile;  /* 128-feature tiles per CTA (1, 2 or 4)                      */
+  int32_t grid;   /* CTA count the measurement used (output)                    */
+  float ms;       /* mean kernel time over the timed repetitions (output)       */
+} dtc_schedule;
+
+/* Fills out[0..min(count, max_out)) with every schedule the kernels support for
+ * N and returns the count (out may be NULL to query it). */
+int dtc_schedule_candidates(int32_t N, dtc_schedule* out, int max_out);
+
+/* Workspace that every candidate's balance mode fits in. */
+dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                        size_t* bytes);
+
+/* Times every candidate (one untimed run + `reps` runs between CUDA events on
+ * `stream`; synchronises it) on the given ME-TCF arrays and B form, writes the
+ * measured schedules to results[0..max_results), their count to *num_results
+ * and the index of the fastest to *best. d_C receives the last candidate's
+ * product. Arguments as in dtc_spmm_ex. */
+dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                        int64_t num_blocks, int bformat, const void* d_Bplane0,
+                        const void* d_Bplane1, int32_t N, int precision, float* d_C,
+                        void* d_workspace, size_t workspace_bytes, int reps,
+                        dtc_schedule* results, int max_results, int* num_results, int* best,
+                        dtc_stream_t stream);
 
 /* d_rowWindowOffset[num_windows+1] from a sorted d_tcblockRowid[T]. */
 dtc_status dtc_rowid_to_window_offset(const int32_t* d_tcblockRowid, int64_t num_blocks,

@@ -169,3 +169,51 @@ def split24_values(hi, ext):
     """fp32 values of the 24-bit form (the B the split kernels multiply)."""
     u = (hi.astype(np.uint32) << 16) | (ext.astype(np.uint32) << 8)
     return u.view(np.float32)
+
+
+def permute_csr(rowptr, col, val, perm):
+    """P A Pᵀ as canonical CSR, restating reordering/TCA_reorder.py:308-326
+    (reorder[i_new] = i_old; d[old] = new; src' = d[src], dst' = d[dst]) and
+    the CSR rebuild of scripts/DTCSpMM/dataset.py:38-44 (scipy coo -> csr:
+    columns sorted per row, duplicates summed). Duplicates are summed in input
+    CSR order; ``val=None`` counts every entry as 1 like the reference."""
+    rowptr = np.asarray(rowptr, np.int64)
+    col = np.asarray(col, np.int64)
+    perm = np.asarray(perm, np.int64)
+    M = len(rowptr) - 1
+    if sorted(perm.tolist()) != list(range(M)):
+        raise ValueError("perm is not a permutation")
+    d = np.empty(M, np.int64)
+    d[perm] = np.arange(M)
+    src = np.repeat(np.arange(M), np.diff(rowptr))
+    return _coo_to_csr(d[src], d[col], val, M, M)
+
+
+def transpose_csr(rowptr, col, val, K):
+    """Aᵀ (K rows) as canonical CSR, duplicates summed in input CSR order."""
+    rowptr = np.asarray(rowptr, np.int64)
+    col = np.asarray(col, np.int64)
+    M = len(rowptr) - 1
+    src = np.repeat(np.arange(M), np.diff(rowptr))
+    return _coo_to_csr(col, src, val, K, M)
+
+
+def _coo_to_csr(r, c, val, rows, cols):
+    nnz = len(r)
+    v = np.ones(nnz, np.float32) if val is None else np.asarray(val, np.float32)
+    order = np.lexsort((np.arange(nnz), c, r))  # stable by (row, col)
+    r, c, v = r[order], c[order], v[order]
+    first = np.ones(nnz, bool)
+    first[1:] = (r[1:] != r[:-1]) | (c[1:] != c[:-1])
+    starts = np.flatnonzero(first)
+    out_v = np.empty(len(starts), np.float32)
+    ends = np.append(starts[1:], nnz)
+    for k, (s, e) in enumerate(zip(starts, ends)):  # sequential float32 sums
+        acc = np.float32(v[s])
+        for j in range(s + 1, e):
+            acc = np.float32(acc + v[j])
+        out_v[k] = acc
+    out_r, out_c = r[starts], c[starts]
+    rp = np.zeros(rows + 1, np.int64)
+    np.add.at(rp, out_r + 1, 1)
+    return np.cumsum(rp).astype(np.int32), out_c.astype(np.int32), out_v

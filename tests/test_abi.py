@@ -53,7 +53,7 @@ def test_bad_arguments_return_status_not_exit():
     assert L.dtc_bformat_bytes(99, 10, 10, C.byref(n), C.byref(n)) == 1
     assert L.dtc_spmm(None, None, None, None, None, 16, 1, 1, None, 16, None, None) == 1
     assert L.dtc_spmm_ex(None, None, None, None, None, 16, 1, 1, 0, None, None, 16, 0, None,
-                         7, 0, None, 0, None) == 1
+                         7, 0, 0, None, 0, None) == 1
 
 
 def test_bformat_sizes():
