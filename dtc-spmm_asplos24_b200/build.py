@@ -25,7 +25,7 @@ EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX")
 
 CU_SOURCES = ["abi.cu", "convert.cu", "spmm_tc.cu", "spmm_split.cu", "spmm_mma.cu", "formats.cu",
               "noalloc.cu", "tune.cu",
-              "relabel.cu"]
+              "relabel.cu", "tca.cu", "features.cu", "mlp.cu"]
 GEN_SOURCES = ["gen.cpp"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", f"-I{INC}", f"-I{CSRC}"]

@@ -2,28 +2,9 @@
 // argument checks, status/error text, per-device state, dispatch.
 #include <mutex>
 #include <string>
-#include "common.cuh"
+#include "impl.h"
 
 namespace dtc {
-
-dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                          const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                          int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile = 0);
-dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                           int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
-                           int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile = 0);
-size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
-dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
-                        cudaStream_t st);
-dtc_status spmm_mma_sync_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                              const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                              const float* B, int32_t N, float* C, cudaStream_t st);
-dtc_status pack_b_impl(int fmt, const float* B, int64_t rows, int32_t N, void* p0, void* p1,
-                       cudaStream_t st);
-dtc_status bformat_bytes_impl(int fmt, int64_t rows, int32_t N, size_t* b0, size_t* b1);
 
 namespace {
 thread_local std::string g_last_error;
@@ -175,6 +156,37 @@ dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, in
   return DTC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+dtc_status spmm_ex_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
+                        const int32_t* s2x, const float* vals, int32_t M, int32_t nwin, int64_t T,
+                        int bformat, const void* p0, const void* p1, int32_t N, int precision,
+                        float* C, int mode, int grid, int ntile, Epilogue epi, void* ws,
+                        size_t wsb, cudaStream_t st) {
+  DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
+  DTC_REQUIRE(grid >= 0, "grid must be >= 0");
+  DTC_REQUIRE(ntile == 0 || ntile == 1 || ntile == 2 || ntile == 4, "ntile must be 0, 1, 2 or 4");
+  DTC_REQUIRE(rwo && toff && p0 && C, "null device pointer");
+  size_t need = 0;
+  dtc_status s = dtc_spmm_ex_workspace_bytes(M, T, N, mode, grid, &need);
+  if (s != DTC_OK) return s;
+  if (need > 0 && (!ws || wsb < need)) {
+    set_error("spmm workspace too small");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
+    return spmm_tf32_impl(rwo, tile, toff, s2x, vals, M, nwin, T, (const float*)p0, N, C, mode,
+                          grid, (float*)ws, st, ntile, epi);
+  return spmm_split_impl(rwo, tile, toff, s2x, vals, M, nwin, T, bformat, p0, p1, N, precision,
+                         C, mode, grid, (float*)ws, st, ntile, epi);
+}
+
+}  // namespace
+
+extern "C" {
+
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
@@ -182,26 +194,26 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
                        const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
                        int grid, int ntile, void* d_workspace, size_t workspace_bytes,
                        dtc_stream_t stream) {
-  DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
-  DTC_REQUIRE(grid >= 0, "grid must be >= 0");
-  DTC_REQUIRE(ntile == 0 || ntile == 1 || ntile == 2 || ntile == 4, "ntile must be 0, 1, 2 or 4");
-  DTC_REQUIRE(d_rowWindowOffset && d_tcblockOffset && d_Bplane0 && d_C, "null device pointer");
-  size_t need = 0;
-  dtc_status s = dtc_spmm_ex_workspace_bytes(num_nodes, num_blocks, N, mode, grid, &need);
-  if (s != DTC_OK) return s;
-  if (need > 0 && (!d_workspace || workspace_bytes < need)) {
-    set_error("spmm workspace too small");
-    return DTC_ERR_WORKSPACE_TOO_SMALL;
-  }
-  cudaStream_t st = (cudaStream_t)stream;
-  if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
-    return spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
-                          d_tcValues, num_nodes, num_windows, num_blocks,
-                          (const float*)d_Bplane0, N, d_C, mode, grid, (float*)d_workspace, st,
-                          ntile);
-  return spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
-                         num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
-                         precision, d_C, mode, grid, (float*)d_workspace, st, ntile);
+  return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
+                      num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
+                      precision, d_C, mode, grid, ntile, Epilogue{}, d_workspace,
+                      workspace_bytes, (cudaStream_t)stream);
+}
+
+dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                          const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                          const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                          int64_t num_blocks, int bformat, const void* d_Bplane0,
+                          const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
+                          int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
+                          size_t workspace_bytes, dtc_stream_t stream) {
+  Epilogue e;
+  e.bias = d_bias;
+  e.relu = relu != 0;
+  return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
+                      num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
+                      precision, d_C, mode, grid, ntile, e, d_workspace, workspace_bytes,
+                      (cudaStream_t)stream);
 }
 
 dtc_status dtc_spmm_mma_sync(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,

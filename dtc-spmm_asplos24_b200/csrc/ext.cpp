@@ -143,13 +143,38 @@ std::vector<torch::Tensor> run_DTCSpMM(torch::Tensor X, torch::Tensor RowWindowO
   return {C};
 }
 
-// DTCSpMM.cpp:147-161 DTCSpMM_gcn (single launch, A = 1).
+// DTCSpMM.cpp:147-161 DTCSpMM_gcn (single launch, A = 1 unless `values`).
+// Optional `bias` [N] and `relu` are fused into the store of C
+// (C = act(A X + bias)), the GCN layer's epilogue.
 std::vector<torch::Tensor> DTCSpMM_gcn(torch::Tensor X, torch::Tensor RowWindowOffset,
                                        torch::Tensor TCblocktileId, torch::Tensor TCblockoffset,
                                        torch::Tensor SparseAToX, int64_t num_nodes,
-                                       int64_t num_edges) {
-  return run_DTCSpMM(X, RowWindowOffset, TCblocktileId, TCblockoffset, SparseAToX, num_nodes,
-                     num_edges, "tcgen05", c10::nullopt);
+                                       int64_t num_edges, c10::optional<torch::Tensor> values,
+                                       c10::optional<torch::Tensor> bias, bool relu) {
+  if (!bias.has_value() && !relu)
+    return run_DTCSpMM(X, RowWindowOffset, TCblocktileId, TCblockoffset, SparseAToX, num_nodes,
+                       num_edges, "tcgen05", values);
+  check_metcf(X, RowWindowOffset, TCblocktileId, TCblockoffset, SparseAToX);
+  const c10::cuda::CUDAGuard guard(X.device());
+  TORCH_CHECK(X.size(0) == num_nodes, "X must have num_nodes rows");
+  const int32_t N = (int32_t)X.size(1);
+  const float* bp = nullptr;
+  if (bias.has_value()) {
+    auto& b = bias.value();
+    CHECK_INPUT(b); CHECK_DTYPE(b, torch::kFloat32);
+    TORCH_CHECK(b.numel() == N, "bias must have N entries");
+    bp = b.data_ptr<float>();
+  }
+  auto C = torch::empty_like(X);
+  const int32_t nwin = (int32_t)RowWindowOffset.numel() - 1;
+  const int64_t T = TCblockoffset.numel() - 1;
+  check(dtc_spmm_fused(RowWindowOffset.data_ptr<int32_t>(), TCblocktileId.data_ptr<uint8_t>(),
+                       TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(),
+                       values_ptr(values, TCblocktileId.numel()), (int32_t)num_nodes, nwin, T,
+                       DTC_B_F32, X.data_ptr<float>(), nullptr, N, DTC_PREC_TF32, bp, relu ? 1 : 0,
+                       C.data_ptr<float>(), 0, 0, 0, nullptr, 0, cur_stream()),
+        "dtc_spmm_fused");
+  return {C};
 }
 
 // DTCSpMM.cpp:163-178 run_DTCSpMM_balance (strict balance, deterministic).
@@ -236,14 +261,20 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("X"), py::arg("TCblockRowid"), py::arg("TCblocktileId"),
         py::arg("TCblockoffset"), py::arg("SparseAToX"), py::arg("num_nodes"),
         py::arg("exeplan"), py::arg("values") = py::none());
-  m.def("DTCSpMM_gcn", &DTCSpMM_gcn, "DTC-SpMM forward for GCN, A = 1 (CUDA)");
+  m.def("DTCSpMM_gcn", &DTCSpMM_gcn, "DTC-SpMM forward for GCN, A = 1 (CUDA)", py::arg("X"),
+        py::arg("RowWindowOffset"), py::arg("TCblocktileId"), py::arg("TCblockoffset"),
+        py::arg("SparseAToX"), py::arg("num_nodes"), py::arg("num_edges"),
+        py::arg("values") = py::none(), py::arg("bias") = py::none(), py::arg("relu") = false);
   // backward aliases of the reference (DTCSpMM.cpp:385-398): the same forward
   // functions, valid as a backward for symmetric A only
   m.def("backward_ptx_uint8_improved", &run_DTCSpMM, "alias of run_DTCSpMM", py::arg("X"),
         py::arg("RowWindowOffset"), py::arg("TCblocktileId"), py::arg("TCblockoffset"),
         py::arg("SparseAToX"), py::arg("num_nodes"), py::arg("num_edges"), py::arg("exeplan"),
         py::arg("values") = py::none());
-  m.def("backward_ptx_uint8_improved_gcn", &DTCSpMM_gcn, "alias of DTCSpMM_gcn");
+  m.def("backward_ptx_uint8_improved_gcn", &DTCSpMM_gcn, "alias of DTCSpMM_gcn", py::arg("X"),
+        py::arg("RowWindowOffset"), py::arg("TCblocktileId"), py::arg("TCblockoffset"),
+        py::arg("SparseAToX"), py::arg("num_nodes"), py::arg("num_edges"),
+        py::arg("values") = py::none(), py::arg("bias") = py::none(), py::arg("relu") = false);
   m.def("balance_backward_ptx_uint8_prefetch", &run_DTCSpMM_balance,
         "alias of run_DTCSpMM_balance", py::arg("X"), py::arg("TCblockRowid"),
         py::arg("TCblocktileId"), py::arg("TCblockoffset"), py::arg("SparseAToX"),

@@ -16,19 +16,8 @@
 // caller. Nothing in the array needs to start at zero: every byte a call reads
 // was written earlier in the same call.
 #include <mutex>
-#include "common.cuh"
+#include "impl.h"
 
-namespace dtc {
-dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                          const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                          int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile = 0);
-dtc_status spmm_mma_sync_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                              const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                              const float* B, int32_t N, float* C, cudaStream_t st);
-dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
-                        cudaStream_t st);
-}  // namespace dtc
 
 namespace {
 

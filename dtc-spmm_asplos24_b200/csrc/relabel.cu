@@ -63,8 +63,20 @@ __global__ void k_rows(const int32_t* __restrict__ rowptr, const int32_t* __rest
   }
 }
 
+// COO input: erow = src, with both coordinates checked against the shape.
+__global__ void k_coo_rows(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                           int32_t M, int32_t K, int64_t nnz, int32_t* __restrict__ erow,
+                           uint32_t* bad) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    const int32_t r = src[e], c = dst[e];
+    if (r < 0 || r >= M || c < 0 || c >= K) atomicOr(bad, 2u);
+    erow[e] = r;
+  }
+}
+
 // key = new_row << colbits | new_col. mode 0: permutation (inv applied to
-// row and column), mode 1: transpose.
+// row and column), mode 1: transpose, mode 2: identity (COO input).
 __global__ void k_keys(const int32_t* __restrict__ erow, const int32_t* __restrict__ col,
                        const int32_t* __restrict__ inv, int64_t nnz, int mode, int colbits,
                        int32_t M, int32_t K, uint64_t* __restrict__ keys,
@@ -76,7 +88,8 @@ __global__ void k_keys(const int32_t* __restrict__ erow, const int32_t* __restri
     c = c < 0 ? 0 : (c >= K ? K - 1 : c);   // a bad input in bounds until the error is read
     uint64_t nr, nc;
     if (mode == 0) { nr = (uint32_t)inv[r]; nc = (uint32_t)inv[c]; }
-    else { nr = (uint32_t)c; nc = (uint32_t)r; }
+    else if (mode == 1) { nr = (uint32_t)c; nc = (uint32_t)r; }
+    else { nr = (uint32_t)r; nc = (uint32_t)c; }
     keys[e] = (nr << colbits) | nc;
     ids[e] = (int32_t)e;
   }
@@ -128,8 +141,8 @@ struct Layout {
 
 Layout layout(int32_t rows_in, int32_t cols_in, int64_t nnz, int mode) {
   Layout L{};
-  const int32_t rows_out = mode == 0 ? rows_in : cols_in;
-  const int32_t cols_out = mode == 0 ? cols_in : rows_in;
+  const int32_t rows_out = mode == 1 ? cols_in : rows_in;
+  const int32_t cols_out = mode == 1 ? rows_in : cols_in;
   L.colbits = bits_for((uint64_t)(cols_out > 0 ? cols_out : 1));
   L.endbit = L.colbits + bits_for((uint64_t)(rows_out > 0 ? rows_out : 1));
   const size_t n = (size_t)(nnz > 0 ? nnz : 1);
@@ -166,9 +179,9 @@ dtc_status relabel(int mode, const int32_t* rowptr, const int32_t* col, const fl
   DTC_REQUIRE(M > 0 || nnz == 0, "a matrix without rows has no entries");
   DTC_REQUIRE(nnz < (int64_t)INT32_MAX, "nnz must fit in int32");
   DTC_REQUIRE(nnz_out != nullptr, "nnz_out is null");
-  DTC_REQUIRE(rowptr && rowptr_out, "null device pointer");
+  DTC_REQUIRE((rowptr || (mode == 2 && nnz == 0)) && rowptr_out, "null device pointer");
   DTC_REQUIRE(nnz == 0 || (col && col_out), "null device pointer");
-  DTC_REQUIRE(mode == 1 || perm || M == 0, "perm is null");
+  DTC_REQUIRE(mode != 0 || perm || M == 0, "perm is null");
   const Layout L = layout(M, K, nnz, mode);
   if (!ws || wsb < L.total) {
     set_error("relabel workspace too small");
@@ -186,13 +199,17 @@ dtc_status relabel(int mode, const int32_t* rowptr, const int32_t* col, const fl
   int32_t* P = (int32_t*)(w + L.P);
   int32_t* rsort = (int32_t*)(w + L.rsort);
   uint32_t* bad = (uint32_t*)(w + L.bad);
-  const int32_t rows_out = mode == 0 ? M : K;
+  const int32_t rows_out = mode == 1 ? K : M;
   DTC_CUDA(cudaMemsetAsync(bad, 0, 4, st));
   if (mode == 0 && M > 0) {
     DTC_CUDA(cudaMemsetAsync(seen, 0, (size_t)M * 4, st));
     k_invert<<<grid_for(M), kThreads, 0, st>>>(perm, M, inv, seen, bad);
   }
-  if (M > 0) k_rows<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow, bad);
+  if (mode == 2) {
+    if (nnz > 0) k_coo_rows<<<grid_for(nnz), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow, bad);
+  } else if (M > 0) {
+    k_rows<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow, bad);
+  }
   uint32_t hbad = 0;
   DTC_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st));
   DTC_CUDA(cudaStreamSynchronize(st));
@@ -201,7 +218,8 @@ dtc_status relabel(int mode, const int32_t* rowptr, const int32_t* col, const fl
     return DTC_ERR_INVALID_ARGUMENT;
   }
   if (hbad & 2u) {
-    set_error("invalid CSR (rowptr not monotone from 0 to nnz, or a column out of range)");
+    set_error(mode == 2 ? "invalid COO (a coordinate out of range)"
+                        : "invalid CSR (rowptr not monotone from 0 to nnz, or a column out of range)");
     return DTC_ERR_INVALID_ARGUMENT;
   }
   if (nnz == 0) {
@@ -238,6 +256,7 @@ dtc_status dtc_relabel_workspace_bytes(int32_t num_rows, int32_t num_cols, int64
                                        size_t* bytes) {
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_rows >= 0 && num_cols >= 0 && nnz >= 0, "negative sizes");
+  // modes 0 and 2 share a layout
   const Layout a = layout(num_rows, num_cols, nnz, 0), b = layout(num_rows, num_cols, nnz, 1);
   *bytes = a.total > b.total ? a.total : b.total;
   return DTC_OK;
@@ -260,6 +279,15 @@ dtc_status dtc_transpose_csr(const int32_t* d_rowptr, const int32_t* d_col, cons
                              dtc_stream_t stream) {
   return relabel(1, d_rowptr, d_col, d_val, num_rows, num_cols, nnz, nullptr, d_rowptr_out,
                  d_col_out, d_val_out, nnz_out, d_workspace, workspace_bytes,
+                 (cudaStream_t)stream);
+}
+
+dtc_status dtc_coo_to_csr(const int32_t* d_src, const int32_t* d_dst, const float* d_val,
+                          int32_t num_rows, int32_t num_cols, int64_t nnz, int32_t* d_rowptr_out,
+                          int32_t* d_col_out, float* d_val_out, int64_t* nnz_out,
+                          void* d_workspace, size_t workspace_bytes, dtc_stream_t stream) {
+  return relabel(2, d_src, d_dst, d_val, num_rows, num_cols, nnz, nullptr,
+                 d_rowptr_out, d_col_out, d_val_out, nnz_out, d_workspace, workspace_bytes,
                  (cudaStream_t)stream);
 }
 

@@ -27,9 +27,17 @@ struct Params {
   float* C;                  // [M x N]
   float* part;               // partial tiles [2*G x 16 x N] (balance mode)
   uint32_t* err;
+  const float* bias;         // epilogue bias [N] or null
+  int32_t relu;              // epilogue ReLU
   int32_t M, nwin, N, G, mode;
   int64_t T;
 };
+
+// The epilogue applied to a finished C element of column f.
+__device__ __forceinline__ float epilogue(const Params& p, float x, int f) {
+  if (p.bias) x += __ldg(p.bias + f);
+  return p.relu ? fmaxf(x, 0.0f) : x;
+}
 
 __device__ __forceinline__ int32_t lower_bound_i32(const int32_t* a, int32_t n, int64_t x) {
   int32_t lo = 0, hi = n;
@@ -112,7 +120,7 @@ __global__ void k_reduce_partials(const Params p) {
     if (row0 + r >= p.M) continue;
     float acc = p.part[(size_t)(2 * (c - 1) + 1) * elems + x];
     for (int k = c; k <= c_last; ++k) acc += p.part[(size_t)(2 * k) * elems + x];
-    p.C[row0 * p.N + x] = acc;
+    p.C[row0 * p.N + x] = epilogue(p, acc, (int)(x - (int64_t)r * p.N));
   }
 }
 

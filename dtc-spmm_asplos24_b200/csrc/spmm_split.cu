@@ -31,6 +31,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "spmm_sched.cuh"
+#include "impl.h"
 
 namespace dtc {
 namespace {
@@ -482,7 +483,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const int64_t row0 = (int64_t)w * kWinH;
       if (r0 == r1) {
         for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
-          for (int r = 0; r < kWinH && row0 + r < p.M; ++r) p.C[(row0 + r) * p.N + f] = 0.0f;
+          for (int r = 0; r < kWinH && row0 + r < p.M; ++r)
+            p.C[(row0 + r) * p.N + f] = epilogue(p, 0.0f, f);
         continue;
       }
       const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
@@ -530,7 +532,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
         if (f < p.N) {
 #pragma unroll
           for (int r = 0; r < kWinH; ++r)
-            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = x[r];
+            if (!guard_rows) out[r * p.N + f] = x[r];  // partial tile: raw sum
+            else if (row0 + r < p.M) out[r * p.N + f] = epilogue(p, x[r], f);
         }
       }
       ++q;
@@ -582,7 +585,7 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile) {
+                           cudaStream_t st, int ntile, Epilogue epi) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8,
               "split kernels take SPLIT24, BF16 or FP8 B");
@@ -606,6 +609,7 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals;
   p.B = reinterpret_cast<const float*>(p0); p.B1 = p1; p.bformat = bformat;
   p.C = C; p.part = part; p.err = device_error_word();
+  p.bias = epi.bias; p.relu = epi.relu;
   p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;

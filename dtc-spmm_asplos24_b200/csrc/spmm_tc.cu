@@ -38,6 +38,7 @@
 // kErrWaitTimeout instead of hanging.
 #include <cuda_bf16.h>
 #include "spmm_sched.cuh"
+#include "impl.h"
 
 namespace dtc {
 namespace {
@@ -299,7 +300,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       const int64_t row0 = (int64_t)w * kWinH;
       if (r0 == r1) {  // empty window: C rows are zero
         for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
-          for (int r = 0; r < kWinH && row0 + r < p.M; ++r) p.C[(row0 + r) * p.N + f] = 0.0f;
+          for (int r = 0; r < kWinH && row0 + r < p.M; ++r)
+            p.C[(row0 + r) * p.N + f] = epilogue(p, 0.0f, f);
         continue;
       }
       if ((r0 > b0 ? r0 : b0) >= (r1 < b1 ? r1 : b1)) continue;
@@ -347,7 +349,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
         if (f < p.N) {
 #pragma unroll
           for (int r = 0; r < kWinH; ++r)
-            if (!guard_rows || row0 + r < p.M) out[r * p.N + f] = x[r];
+            if (!guard_rows) out[r * p.N + f] = x[r];  // partial tile: raw sum
+            else if (row0 + r < p.M) out[r * p.N + f] = epilogue(p, x[r], f);
         }
       }
       ++q;
@@ -400,7 +403,7 @@ dtc_status launch_tf32(const Params& p, int slices, cudaStream_t st) {
 dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile) {
+                          float* part, cudaStream_t st, int ntile, Epilogue epi) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0 (16-byte row segments)");
   DTC_REQUIRE(((uintptr_t)B & 15) == 0, "B must be 16-byte aligned");
@@ -417,6 +420,7 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
   Params p{};
   p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals; p.B = B;
   p.C = C; p.part = part; p.err = device_error_word();
+  p.bias = epi.bias; p.relu = epi.relu;
   p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;

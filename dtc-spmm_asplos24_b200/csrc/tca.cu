@@ -1,0 +1,461 @@
+// TCA reorder: two-level MinHash-LSH + Jaccard clustering of rows
+// (reordering/TCA_reorder.py:53-326), producing the permutation that packs
+// rows with similar column sets into the same row windows.
+//
+// Level 1 ("TCU-aware", :53-241): rows are items, each with its column set.
+// Level 2 ("cache-aware", :243-305): the level-1 clusters are items, each with
+// the union of its rows' column sets. At each level:
+//   1. MinHash signatures, `num_perm` hash functions (GPU; a cluster's
+//      signature is the element-wise min of its rows' signatures, which is the
+//      MinHash of the union).
+//   2. LSH banding: `bands` bands of `rows_per_band` signature values; items
+//      whose band values all agree share a bucket (GPU radix sort of
+//      (band, band-hash) keys). Each item is paired with the next
+//      `bucket_window` items of its bucket (the reference pairs every bucket
+//      member; the window bounds hub buckets).
+//   3. Exact Jaccard similarity of every distinct candidate pair (host).
+//   4. Greedy merging by descending similarity with union-find, exactly the
+//      reference's loop (:171-205 / :268-293): two live roots merge (smaller
+//      size into larger; ties into the first of the pair); a cluster whose
+//      size reaches the cap (`thres` rows at level 1, `c_thres` clusters at
+//      level 2) stops merging; a pair whose ends are no longer roots is
+//      requeued once as (root, root) with the Jaccard of the two roots' own
+//      item sets. Ties in similarity pop in (first, second) order.
+// Clusters are numbered in order of their smallest member, members ascending;
+// the output lists level-2 groups in that order, each group's clusters in
+// ascending number and each cluster's rows ascending (:308-315).
+// Items with an empty set never enter LSH and stay singletons.
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <queue>
+#include <unordered_set>
+#include <vector>
+#include "common.cuh"
+
+namespace dtc {
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(int64_t n) {
+  int64_t g = (n + kThreads - 1) / kThreads;
+  if (g < 1) g = 1;
+  if (g > (1 << 30)) g = 1 << 30;
+  return (unsigned)g;
+}
+
+// splitmix64 finaliser (Steele, Lea, Flood 2014): a bijective 64-bit mixer.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// sig[i * P + k] = min over columns c of row i of h_k(c), where h_k(c) is the
+// high 32 bits of mix64(c ^ salt_k), salt_k = mix64(seed + 0x9e37...15 * (k+1));
+// rows without columns keep 0xffffffff. One warp per row, lanes over k.
+__global__ void k_row_signatures(const int32_t* __restrict__ rowptr,
+                                 const int32_t* __restrict__ col, int32_t M, int P,
+                                 uint64_t seed, uint32_t* __restrict__ sig) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < M; r += nwarps) {
+    const int32_t e0 = rowptr[r], e1 = rowptr[r + 1];
+    for (int k = lane; k < P; k += 32) {
+      uint64_t salt = mix64(seed + 0x9e3779b97f4a7c15ull * (uint64_t)(k + 1));
+      uint32_t m = 0xffffffffu;
+      for (int32_t e = e0; e < e1; ++e) {
+        const uint32_t h = (uint32_t)(mix64((uint64_t)(uint32_t)col[e] ^ salt) >> 32);
+        m = h < m ? h : m;
+      }
+      sig[r * P + k] = m;
+    }
+  }
+}
+
+// Cluster signatures: element-wise min over member rows (cid[row] = cluster).
+__global__ void k_cluster_signatures(const uint32_t* __restrict__ rsig,
+                                     const int32_t* __restrict__ cid, int32_t M, int P,
+                                     uint32_t* __restrict__ csig) {
+  const int64_t n = (int64_t)M * P;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int32_t r = (int32_t)(i / P);
+    const int k = (int)(i % P);
+    const uint32_t v = rsig[i];
+    if (v != 0xffffffffu) atomicMin(csig + (int64_t)cid[r] * P + k, v);
+  }
+}
+
+// Band keys: key = band << 40 | 40 bits of the hash of the band's values.
+// Items with an empty set get the sentinel key ~0 (sorted last, never paired).
+__global__ void k_band_keys(const uint32_t* __restrict__ sig, int32_t n, int P, int bands,
+                            int rpb, uint64_t* __restrict__ keys, int32_t* __restrict__ items) {
+  const int64_t total = (int64_t)n * bands;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += stride) {
+    const int b = (int)(t / n);
+    const int32_t i = (int32_t)(t % n);
+    const uint32_t* s = sig + (int64_t)i * P + b * rpb;
+    uint64_t h = 0x51ed27a3c0ffee11ull ^ (uint64_t)b;
+    bool empty = false;
+    for (int j = 0; j < rpb; ++j) {
+      empty |= (s[j] == 0xffffffffu);
+      h = mix64(h ^ s[j]);
+    }
+    keys[t] = empty ? ~0ull : (((uint64_t)b << 40) | (h & ((1ull << 40) - 1)));
+    items[t] = i;
+  }
+}
+
+// Pairs of each sorted position with the next `win` positions of its bucket:
+// pass 0 counts, pass 1 writes (lo << 32 | hi) at the scanned offsets.
+__global__ void k_bucket_pairs(const uint64_t* __restrict__ keys, const int32_t* __restrict__ items,
+                               int64_t n, int win, int32_t* __restrict__ counts,
+                               const int32_t* __restrict__ offs, uint64_t* __restrict__ pairs) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += stride) {
+    const uint64_t k = keys[p];
+    int c = 0;
+    if (k != ~0ull) {
+      for (int q = 1; q <= win && p + q < n && keys[p + q] == k; ++q) {
+        if (pairs) {
+          uint32_t a = (uint32_t)items[p], b = (uint32_t)items[p + q];
+          if (a > b) { uint32_t t = a; a = b; b = t; }
+          pairs[offs[p] + c] = ((uint64_t)a << 32) | b;
+        }
+        ++c;
+      }
+    }
+    if (!pairs) counts[p] = c;
+  }
+}
+
+// Device workspace for one level over n items with P-value signatures.
+struct LshLayout {
+  size_t keys_in, keys_out, items_in, items_out, counts, offs, pairs_in, pairs_out, sort1, scan,
+      sort2, total;
+};
+
+LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
+  LshLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t b) { size_t o = off; off = align_up(off + (b ? b : 1), 256); return o; };
+  const size_t n = (size_t)(n_keys > 0 ? n_keys : 1);
+  const size_t mp = (size_t)(max_pairs > 0 ? max_pairs : 1);
+  L.keys_in = take(n * 8);
+  L.keys_out = take(n * 8);
+  L.items_in = take(n * 4);
+  L.items_out = take(n * 4);
+  L.counts = take((n + 1) * 4);
+  L.offs = take((n + 1) * 4);
+  L.pairs_in = take(mp * 8);
+  L.pairs_out = take(mp * 8);
+  size_t s1 = 0, s2 = 0, s3 = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, s1, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                  (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n);
+  cub::DeviceScan::ExclusiveSum(nullptr, s2, (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n + 1);
+  cub::DeviceRadixSort::SortKeys(nullptr, s3, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)mp);
+  L.sort1 = take(s1);
+  L.scan = take(s2);
+  L.sort2 = take(s3);
+  L.total = off;
+  return L;
+}
+
+// Candidate pairs (lo, hi), lo < hi, sorted and distinct, for n items.
+dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, char* ws,
+                     const LshLayout& L, int64_t max_pairs, cudaStream_t st,
+                     std::vector<uint64_t>& out) {
+  out.clear();
+  if (n < 2) return DTC_OK;
+  const int64_t nk = (int64_t)n * prm.bands;
+  uint64_t* kin = (uint64_t*)(ws + L.keys_in);
+  uint64_t* kout = (uint64_t*)(ws + L.keys_out);
+  int32_t* iin = (int32_t*)(ws + L.items_in);
+  int32_t* iout = (int32_t*)(ws + L.items_out);
+  int32_t* counts = (int32_t*)(ws + L.counts);
+  int32_t* offs = (int32_t*)(ws + L.offs);
+  uint64_t* pin = (uint64_t*)(ws + L.pairs_in);
+  uint64_t* pout = (uint64_t*)(ws + L.pairs_out);
+  k_band_keys<<<grid_for(nk), kThreads, 0, st>>>(sig, n, prm.num_perm, prm.bands,
+                                                 prm.rows_per_band, kin, iin);
+  size_t b1 = L.scan - L.sort1;
+  DTC_CUDA(cub::DeviceRadixSort::SortPairs(ws + L.sort1, b1, kin, kout, iin, iout, nk, 0, 64, st));
+  k_bucket_pairs<<<grid_for(nk), kThreads, 0, st>>>(kout, iout, nk, prm.bucket_window, counts,
+                                                    nullptr, nullptr);
+  DTC_CUDA(cudaMemsetAsync(counts + nk, 0, 4, st));
+  size_t b2 = L.sort2 - L.scan;
+  DTC_CUDA(cub::DeviceScan::ExclusiveSum(ws + L.scan, b2, counts, offs, nk + 1, st));
+  int32_t np = 0;
+  DTC_CUDA(cudaMemcpyAsync(&np, offs + nk, 4, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaStreamSynchronize(st));
+  if (np <= 0) return DTC_OK;
+  if (np > max_pairs) {
+    set_error("tca: candidate pairs exceed the workspace bound");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  k_bucket_pairs<<<grid_for(nk), kThreads, 0, st>>>(kout, iout, nk, prm.bucket_window, counts,
+                                                    offs, pin);
+  size_t b3 = L.total - L.sort2;
+  DTC_CUDA(cub::DeviceRadixSort::SortKeys(ws + L.sort2, b3, pin, pout, (int64_t)np, 0, 64, st));
+  std::vector<uint64_t> h(np);
+  DTC_CUDA(cudaMemcpyAsync(h.data(), pout, (size_t)np * 8, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaStreamSynchronize(st));
+  out.reserve(np);
+  for (int32_t i = 0; i < np; ++i)
+    if (i == 0 || h[i] != h[i - 1]) out.push_back(h[i]);
+  return DTC_OK;
+}
+
+// Jaccard |a ∩ b| / |a ∪ b| of two sorted, distinct lists (0 when either is empty).
+double jaccard(const int32_t* a, int64_t na, const int32_t* b, int64_t nb) {
+  if (na == 0 || nb == 0) return 0.0;
+  int64_t i = 0, j = 0, inter = 0;
+  while (i < na && j < nb) {
+    if (a[i] < b[j]) ++i;
+    else if (a[i] > b[j]) ++j;
+    else { ++inter; ++i; ++j; }
+  }
+  return (double)inter / (double)(na + nb - inter);
+}
+
+// Item sets as CSR of sorted distinct members.
+struct Sets {
+  std::vector<int64_t> ptr;
+  std::vector<int32_t> idx;
+  double jac(int32_t a, int32_t b) const {
+    return jaccard(idx.data() + ptr[a], ptr[a + 1] - ptr[a], idx.data() + ptr[b],
+                   ptr[b + 1] - ptr[b]);
+  }
+};
+
+struct QItem {
+  double s;
+  int32_t a, b;
+  bool operator<(const QItem& o) const {  // max-heap on s, then (a, b) ascending
+    if (s != o.s) return s < o.s;
+    if (a != o.a) return a > o.a;
+    return b > o.b;
+  }
+};
+
+// The greedy merge loop; returns the root of every item.
+std::vector<int32_t> greedy_merge(const Sets& sets, const std::vector<uint64_t>& pairs,
+                                  int32_t n, int32_t cap) {
+  std::vector<int32_t> parent(n), size(n, 1);
+  std::vector<char> deleted(n, 0);
+  for (int32_t i = 0; i < n; ++i) parent[i] = i;
+  auto root = [&](int32_t i) {
+    while (i != parent[i]) {
+      parent[i] = parent[parent[i]];
+      i = parent[i];
+    }
+    return i;
+  };
+  std::priority_queue<QItem> q;
+  std::unordered_set<uint64_t> inset;  // pairs currently queued (lo << 32 | hi)
+  inset.reserve(pairs.size() * 2 + 16);
+  auto key = [](int32_t a, int32_t b) {
+    return a < b ? ((uint64_t)a << 32) | (uint32_t)b : ((uint64_t)b << 32) | (uint32_t)a;
+  };
+  for (uint64_t p : pairs) {
+    const int32_t a = (int32_t)(p >> 32), b = (int32_t)(p & 0xffffffffu);
+    q.push({sets.jac(a, b), a, b});
+    inset.insert(p);
+  }
+  int64_t num_cluster = n;
+  while (!q.empty() && num_cluster > 0) {
+    const QItem it = q.top();
+    q.pop();
+    int32_t p1 = it.a, p2 = it.b;
+    inset.erase(key(p1, p2));
+    if (p1 == parent[p1] && p2 == parent[p2]) {
+      if (deleted[p1] || deleted[p2]) continue;
+      if (size[p1] < size[p2]) {
+        parent[p1] = p2;
+        --num_cluster;
+        size[p2] += size[p1];
+        if (size[p2] >= cap) { deleted[p2] = 1; --num_cluster; }
+      } else {
+        parent[p2] = p1;
+        --num_cluster;
+        size[p1] += size[p2];
+        if (size[p1] >= cap) { deleted[p1] = 1; --num_cluster; }
+      }
+    } else {
+      p1 = root(p1);
+      p2 = root(p2);
+      if (deleted[p1] || deleted[p2]) continue;
+      if (p1 != p2 && !inset.count(key(p1, p2))) {
+        q.push({sets.jac(p1, p2), p1, p2});
+        inset.insert(key(p1, p2));
+      }
+    }
+  }
+  std::vector<int32_t> r(n);
+  for (int32_t i = 0; i < n; ++i) r[i] = root(i);
+  return r;
+}
+
+// Groups items by root in order of first appearance; members ascending.
+std::vector<std::vector<int32_t>> groups_of(const std::vector<int32_t>& roots) {
+  const int32_t n = (int32_t)roots.size();
+  std::vector<int32_t> gid(n, -1);
+  std::vector<std::vector<int32_t>> g;
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t r = roots[i];
+    if (gid[r] < 0) { gid[r] = (int32_t)g.size(); g.emplace_back(); }
+    g[gid[r]].push_back(i);
+  }
+  return g;
+}
+
+dtc_tca_params defaults() {
+  dtc_tca_params p{};
+  p.num_perm = 128;
+  p.bands = 42;
+  p.rows_per_band = 3;
+  p.thres = 16;
+  p.c_thres = 128;
+  p.bucket_window = 8;
+  p.seed = 2022;
+  return p;
+}
+
+}  // namespace
+}  // namespace dtc
+
+using namespace dtc;
+
+extern "C" {
+
+void dtc_tca_default_params(dtc_tca_params* p) {
+  if (p) *p = defaults();
+}
+
+dtc_status dtc_tca_workspace_bytes(int32_t num_nodes, int64_t nnz, const dtc_tca_params* params,
+                                   size_t* bytes) {
+  DTC_REQUIRE(bytes != nullptr, "bytes is null");
+  DTC_REQUIRE(num_nodes >= 0 && nnz >= 0, "negative sizes");
+  const dtc_tca_params p = params ? *params : defaults();
+  DTC_REQUIRE(p.num_perm >= 1 && p.bands >= 1 && p.rows_per_band >= 1 &&
+                  p.bands * p.rows_per_band <= p.num_perm,
+              "need bands * rows_per_band <= num_perm");
+  DTC_REQUIRE(p.bucket_window >= 1 && p.bucket_window <= 64, "bucket_window must be in [1, 64]");
+  const int64_t n = num_nodes > 0 ? num_nodes : 1;
+  const int64_t nk = n * p.bands;
+  DTC_REQUIRE(nk * p.bucket_window < (int64_t)INT32_MAX,
+              "num_nodes * bands * bucket_window must fit in int32");
+  const LshLayout L = lsh_layout(nk, nk * p.bucket_window);
+  size_t off = align_up((size_t)n * p.num_perm * 4, 256) * 2;  // row + cluster signatures
+  off += align_up((size_t)n * 4, 256);                          // cluster id per row
+  *bytes = off + L.total;
+  return DTC_OK;
+}
+
+dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_t num_nodes,
+                           int64_t nnz, const dtc_tca_params* params, int32_t* d_perm,
+                           void* d_workspace, size_t workspace_bytes, dtc_stream_t stream) {
+  DTC_REQUIRE(num_nodes >= 0 && nnz >= 0, "negative sizes");
+  DTC_REQUIRE(d_rowptr && d_perm, "null device pointer");
+  DTC_REQUIRE(nnz == 0 || d_col, "null device pointer");
+  const dtc_tca_params p = params ? *params : defaults();
+  DTC_REQUIRE(p.thres >= 1 && p.c_thres >= 1, "cluster caps must be >= 1");
+  size_t need = 0;
+  dtc_status s = dtc_tca_workspace_bytes(num_nodes, nnz, &p, &need);
+  if (s != DTC_OK) return s;
+  if (!d_workspace || workspace_bytes < need) {
+    set_error("tca workspace too small");
+    return DTC_ERR_WORKSPACE_TOO_SMALL;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const int32_t M = num_nodes;
+  if (M == 0) return DTC_OK;
+  // host copy of the rows' column sets (sorted, distinct)
+  std::vector<int32_t> hrp(M + 1), hcol(nnz);
+  DTC_CUDA(cudaMemcpyAsync(hrp.data(), d_rowptr, (size_t)(M + 1) * 4, cudaMemcpyDeviceToHost, st));
+  if (nnz)
+    DTC_CUDA(cudaMemcpyAsync(hcol.data(), d_col, (size_t)nnz * 4, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaStreamSynchronize(st));
+  if (hrp[0] != 0 || hrp[M] != nnz) {
+    set_error("tca: rowptr must run from 0 to nnz");
+    return DTC_ERR_INVALID_ARGUMENT;
+  }
+  Sets rows;
+  rows.ptr.resize(M + 1);
+  rows.idx.reserve(nnz);
+  rows.ptr[0] = 0;
+  for (int32_t r = 0; r < M; ++r) {
+    if (hrp[r + 1] < hrp[r]) {
+      set_error("tca: rowptr must be non-decreasing");
+      return DTC_ERR_INVALID_ARGUMENT;
+    }
+    std::vector<int32_t> v(hcol.begin() + hrp[r], hcol.begin() + hrp[r + 1]);
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    for (int32_t c : v)
+      if (c < 0 || c >= M) {
+        set_error("tca: column index out of range");
+        return DTC_ERR_INVALID_ARGUMENT;
+      }
+    rows.idx.insert(rows.idx.end(), v.begin(), v.end());
+    rows.ptr[r + 1] = (int64_t)rows.idx.size();
+  }
+  char* ws = (char*)d_workspace;
+  const size_t sig_bytes = align_up((size_t)M * p.num_perm * 4, 256);
+  uint32_t* rsig = (uint32_t*)ws;
+  uint32_t* csig = (uint32_t*)(ws + sig_bytes);
+  int32_t* cid = (int32_t*)(ws + 2 * sig_bytes);
+  char* lws = ws + 2 * sig_bytes + align_up((size_t)M * 4, 256);
+  const int64_t nk = (int64_t)M * p.bands;
+  const int64_t max_pairs = nk * p.bucket_window;
+  const LshLayout L = lsh_layout(nk, max_pairs);
+
+  // ---- level 1: rows
+  k_row_signatures<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(d_rowptr, d_col, M, p.num_perm,
+                                                                   p.seed, rsig);
+  DTC_CUDA(cudaGetLastError());
+  std::vector<uint64_t> pairs;
+  s = lsh_pairs(rsig, M, p, lws, L, max_pairs, st, pairs);
+  if (s != DTC_OK) return s;
+  const auto groups1 = groups_of(greedy_merge(rows, pairs, M, p.thres));
+  const int32_t nc = (int32_t)groups1.size();
+
+  // ---- level 2: clusters, each with the union of its rows' sets
+  std::vector<int32_t> hcid(M);
+  Sets cl;
+  cl.ptr.resize(nc + 1);
+  cl.ptr[0] = 0;
+  for (int32_t c = 0; c < nc; ++c) {
+    std::vector<int32_t> u;
+    for (int32_t r : groups1[c]) {
+      hcid[r] = c;
+      u.insert(u.end(), rows.idx.begin() + rows.ptr[r], rows.idx.begin() + rows.ptr[r + 1]);
+    }
+    std::sort(u.begin(), u.end());
+    u.erase(std::unique(u.begin(), u.end()), u.end());
+    cl.idx.insert(cl.idx.end(), u.begin(), u.end());
+    cl.ptr[c + 1] = (int64_t)cl.idx.size();
+  }
+  DTC_CUDA(cudaMemcpyAsync(cid, hcid.data(), (size_t)M * 4, cudaMemcpyHostToDevice, st));
+  DTC_CUDA(cudaMemsetAsync(csig, 0xff, (size_t)nc * p.num_perm * 4, st));
+  k_cluster_signatures<<<grid_for((int64_t)M * p.num_perm), kThreads, 0, st>>>(rsig, cid, M,
+                                                                              p.num_perm, csig);
+  DTC_CUDA(cudaGetLastError());
+  s = lsh_pairs(csig, nc, p, lws, L, max_pairs, st, pairs);
+  if (s != DTC_OK) return s;
+  const auto groups2 = groups_of(greedy_merge(cl, pairs, nc, p.c_thres));
+
+  std::vector<int32_t> perm;
+  perm.reserve(M);
+  for (const auto& g : groups2)
+    for (int32_t c : g)
+      for (int32_t r : groups1[c]) perm.push_back(r);
+  DTC_CUDA(cudaMemcpyAsync(d_perm, perm.data(), (size_t)M * 4, cudaMemcpyHostToDevice, st));
+  DTC_CUDA(cudaStreamSynchronize(st));
+  return DTC_OK;
+}
+
+}  // extern "C"

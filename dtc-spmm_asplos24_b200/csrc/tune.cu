@@ -16,20 +16,8 @@
 // candidate's result is bitwise reproducible (window mode writes every C
 // element once, balance mode reduces its partial tiles in fixed order).
 #include <vector>
-#include "common.cuh"
+#include "impl.h"
 
-namespace dtc {
-dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                          const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                          int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile);
-dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
-                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
-                           int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
-                           int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile);
-size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
-}  // namespace dtc
 
 using namespace dtc;
 

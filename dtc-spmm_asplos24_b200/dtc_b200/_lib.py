@@ -36,20 +36,48 @@ SIGNATURES = {
     "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
                     C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, C.c_int, C.c_int, szp],
+    "dtc_spmm_fused": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
+                       C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
     "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
     "dtc_spmm_balance_noalloc": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp],
     "dtc_noalloc_scratch_capacity": [],
     "dtc_schedule_candidates": [i32, vp, C.c_int],
     "dtc_relabel_workspace_bytes": [i32, i32, i64, szp],
+    "dtc_tca_default_params": [vp],
+    "dtc_features_workspace_bytes": [],
+    "dtc_features": [vp, vp, i32, i64, vp, vp, vp, i32, i64, i32, vp, vp, sz, vp],
+    "dtc_mlp_num_params": [vp],
+    "dtc_mlp_forward": [vp, vp, vp, i32, vp, vp, vp, vp],
+    "dtc_mlp_backward_workspace_bytes": [vp, i32],
+    "dtc_mlp_backward": [vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, sz, vp],
+    "dtc_mlp_adam": [vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i32, vp],
+    "dtc_mlp_argmin": [vp, vp, C.c_int, i32, i32, vp, vp],
+    "dtc_tca_workspace_bytes": [i32, i64, vp, szp],
+    "dtc_tca_reorder": [vp, vp, i32, i64, vp, vp, vp, sz, vp],
     "dtc_permute_csr": [vp, vp, vp, i32, i64, vp, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_transpose_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
+    "dtc_coo_to_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_autotune_workspace_bytes": [i32, i64, i32, szp],
     "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp, vp, sz,
                      C.c_int, vp, C.c_int, vp, vp, vp],
 }
 _RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int,
-             "dtc_noalloc_scratch_capacity": C.c_size_t, "dtc_schedule_candidates": C.c_int}
+             "dtc_noalloc_scratch_capacity": C.c_size_t, "dtc_schedule_candidates": C.c_int,
+             "dtc_tca_default_params": None, "dtc_features_workspace_bytes": C.c_size_t,
+             "dtc_mlp_num_params": C.c_int64, "dtc_mlp_backward_workspace_bytes": C.c_size_t}
+
+
+class MlpDims(C.Structure):
+    """dtc_mlp_dims (include/dtc_spmm.h)."""
+    _fields_ = [("in_", C.c_int32), ("h1", C.c_int32), ("h2", C.c_int32), ("out", C.c_int32)]
+
+
+class TcaParams(C.Structure):
+    """dtc_tca_params (include/dtc_spmm.h)."""
+    _fields_ = [("num_perm", C.c_int32), ("bands", C.c_int32), ("rows_per_band", C.c_int32),
+                ("thres", C.c_int32), ("c_thres", C.c_int32), ("bucket_window", C.c_int32),
+                ("seed", C.c_uint64)]
 
 
 class Schedule(C.Structure):

@@ -1,0 +1,411 @@
+"""Learned schedule cost model: features (dtc_features) -> MLP 48 -> 64 -> 64 -> K
+(dtc_mlp_* kernels) -> the schedule class with the lowest predicted cost.
+
+The reference fixes its schedule by hand per dataset and N
+(scripts/DTCSpMM/run_DTC_SpMM.py:10-30). Here a class is one full choice
+
+    (window height, compaction width, mode, waves, N-tile, B form, reorder)
+
+with window 16 x width 8 TC blocks, mode 0 (window-scheduled) or 1 (strict
+balance; the split threshold is ceil(T / CTAs) blocks), waves in {1,2,4,8,16}
+(CTAs = waves x SMs), N-tiles per CTA in {1,2,4}, the two B forms within
+1e-5 relative error (SPLIT24 with 4- or 3-term products) and TCA reorder off or
+on. The network predicts, for every class, log(t_class / t_best) of the SpMM
+kernel; it is trained on timings the library measures itself on seeded
+synthetic matrices (``collect``), entirely with the library's own CUDA kernels
+(forward, backward, Adam). The model changes only which schedule runs: every
+class computes the same product within its form's error bound. The exhaustive
+autotuner (``tune.autotune`` over every class) is its fallback and the
+reference point of its regret.
+"""
+import ctypes as C
+import math
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib, gen, metcf, reorder as reorder_mod, tune
+from ._lib import MlpDims, call
+from .metcf import _ptr, _stream
+
+NFEAT = 48
+WAVES = (1, 2, 4, 8, 16)
+NTILES = (1, 2, 4)
+FORMS = ("split24x4", "split24x3")
+CLASSES = [dict(H=16, W=8, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
+           for ro in (0, 1) for fo in FORMS for mo in (0, 1) for wv in WAVES for nt in NTILES]
+K = len(CLASSES)
+DEFAULT_CLASS = next(i for i, c in enumerate(CLASSES)
+                     if c["mode"] == 1 and c["waves"] == 16 and c["ntile"] == 1
+                     and c["form"] == "split24x4" and c["reorder"] == 0)
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+DATASET_PATH = os.path.join(DATA_DIR, "costmodel_dataset.npz")
+WEIGHTS_PATH = os.path.join(DATA_DIR, "costmodel_weights.npz")
+
+
+def auto_ntile(N):
+    return 1 if N <= 128 else 2 if N <= 256 else 4
+
+
+def feasible(N):
+    """uint8 [K]: classes whose N-tile the kernels run for width N."""
+    return np.array([c["ntile"] <= auto_ntile(N) for c in CLASSES], np.uint8)
+
+
+def class_of(mode, waves, ntile, form, reorder):
+    for i, c in enumerate(CLASSES):
+        if (c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"]) == \
+                (mode, waves, ntile, form, reorder):
+            return i
+    raise KeyError((mode, waves, ntile, form, reorder))
+
+
+def default_class(N):
+    """The untuned library default for width N (strict balance, 16 waves, all
+    N-tiles in one CTA, SPLIT24 4-term, no reorder)."""
+    return class_of(1, 16, auto_ntile(N), "split24x4", 0)
+
+
+# ----------------------------------------------------------------- features
+def features(rowptr, col, m: metcf.METCF, N):
+    """float32 [48] device tensor of dtc_features for CSR (device) + its METCF."""
+    dev = m.RowWindowOffset.device
+    rowptr = rowptr.to(dev, torch.int32).contiguous()
+    col = col.to(dev, torch.int32).contiguous()
+    out = torch.empty(NFEAT, dtype=torch.float32, device=dev)
+    wsb = _lib.lib().dtc_features_workspace_bytes()
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    call("dtc_features", _ptr(rowptr), _ptr(col), m.M, col.numel(), _ptr(m.RowWindowOffset),
+         _ptr(m.TCblockoffset), _ptr(m.edgeToColumn), m.nwin, m.T, N, _ptr(out), _ptr(ws),
+         wsb, _stream())
+    return out
+
+
+# ---------------------------------------------------------------------- MLP
+class MLP:
+    """48 -> 64 -> 64 -> K network whose every pass runs in libdtcspmm.so."""
+
+    def __init__(self, dims=(NFEAT, 64, 64, K), seed=0, device="cuda", params=None):
+        self.dims = tuple(int(d) for d in dims)
+        self.cd = MlpDims(*self.dims)
+        n = _lib.lib().dtc_mlp_num_params(C.byref(self.cd))
+        if n < 0:
+            raise ValueError(f"bad MLP dims {dims}")
+        self.n = n
+        self.device = torch.device(device)
+        if params is None:
+            params = self.init_params(seed)
+        self.params = torch.as_tensor(np.asarray(params, np.float32)).to(self.device).contiguous()
+        assert self.params.numel() == n
+
+    def init_params(self, seed):
+        """He-uniform weights, zero biases (numpy, seeded)."""
+        rng = np.random.default_rng(seed)
+        i, h1, h2, o = self.dims
+        parts = []
+        for fan_in, fan_out in ((i, h1), (h1, h2), (h2, o)):
+            lim = math.sqrt(6.0 / fan_in)
+            parts.append(rng.uniform(-lim, lim, fan_in * fan_out))
+            parts.append(np.zeros(fan_out))
+        return np.concatenate(parts).astype(np.float32)
+
+    def _acts(self, B):
+        i, h1, h2, o = self.dims
+        e = lambda w: torch.empty((max(B, 1), w), dtype=torch.float32, device=self.device)
+        return e(h1), e(h2), e(o)
+
+    def forward(self, X):
+        X = torch.as_tensor(X, dtype=torch.float32).to(self.device).contiguous()
+        B = X.shape[0]
+        H1, H2, Y = self._acts(B)
+        call("dtc_mlp_forward", C.byref(self.cd), _ptr(self.params), _ptr(X), B, _ptr(H1),
+             _ptr(H2), _ptr(Y), _stream())
+        return H1[:B], H2[:B], Y[:B]
+
+    def loss_and_grads(self, X, target, mask):
+        X = torch.as_tensor(X, dtype=torch.float32).to(self.device).contiguous()
+        target = torch.as_tensor(target, dtype=torch.float32).to(self.device).contiguous()
+        mask = torch.as_tensor(mask, dtype=torch.float32).to(self.device).contiguous()
+        B = X.shape[0]
+        H1, H2, Y = self.forward(X)
+        grads = torch.empty(self.n, dtype=torch.float32, device=self.device)
+        loss = torch.empty(1, dtype=torch.float32, device=self.device)
+        wsb = _lib.lib().dtc_mlp_backward_workspace_bytes(C.byref(self.cd), B)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=self.device)
+        call("dtc_mlp_backward", C.byref(self.cd), _ptr(self.params), _ptr(X), _ptr(H1),
+             _ptr(H2), _ptr(Y), _ptr(target), _ptr(mask), B, _ptr(grads), _ptr(loss), _ptr(ws),
+             wsb, _stream())
+        return loss, grads
+
+    def train(self, X, target, mask, steps=3000, lr=2e-3, beta1=0.9, beta2=0.999, eps=1e-8,
+              batch=None, seed=0, log_every=0):
+        """Adam on the masked MSE; full batch unless ``batch`` is given."""
+        X = torch.as_tensor(X, dtype=torch.float32).to(self.device).contiguous()
+        T = torch.as_tensor(target, dtype=torch.float32).to(self.device).contiguous()
+        Mk = torch.as_tensor(mask, dtype=torch.float32).to(self.device).contiguous()
+        m = torch.zeros(self.n, dtype=torch.float32, device=self.device)
+        v = torch.zeros_like(m)
+        rng = np.random.default_rng(seed)
+        S = X.shape[0]
+        hist = []
+        for step in range(1, steps + 1):
+            if batch and batch < S:
+                idx = torch.as_tensor(rng.choice(S, batch, replace=False), device=self.device)
+                xb, tb, mb = X[idx].contiguous(), T[idx].contiguous(), Mk[idx].contiguous()
+            else:
+                xb, tb, mb = X, T, Mk
+            loss, g = self.loss_and_grads(xb, tb, mb)
+            call("dtc_mlp_adam", _ptr(self.params), _ptr(g), _ptr(m), _ptr(v), self.n, lr, beta1,
+                 beta2, eps, step, _stream())
+            if log_every and (step % log_every == 0 or step == 1):
+                hist.append((step, float(loss.item())))
+        return hist
+
+    def choose(self, X, feas):
+        """Class index with the lowest predicted cost among feasible ones, per row."""
+        _, _, Y = self.forward(X)
+        B = Y.shape[0]
+        feas = torch.as_tensor(np.asarray(feas, np.uint8)).to(self.device).contiguous()
+        per_row = 1 if feas.dim() == 2 else 0
+        ch = torch.empty(max(B, 1), dtype=torch.int32, device=self.device)
+        call("dtc_mlp_argmin", _ptr(Y.contiguous()), _ptr(feas), per_row, B, self.dims[3],
+             _ptr(ch), _stream())
+        return ch[:B].cpu().numpy()
+
+    def save(self, path, **meta):
+        np.savez(path, params=self.params.cpu().numpy(), dims=np.array(self.dims), **meta)
+
+    @classmethod
+    def load(cls, path, device="cuda"):
+        z = np.load(path)
+        return cls(dims=tuple(z["dims"]), params=z["params"], device=device)
+
+
+# -------------------------------------------------------- training targets
+def targets(times):
+    """times [S, K] ms (NaN = not measured) -> (log(t / t_best), mask)."""
+    t = np.asarray(times, np.float64)
+    ok = np.isfinite(t) & (t > 0)
+    best = np.where(ok, t, np.inf).min(axis=1, keepdims=True)
+    y = np.where(ok, np.log(np.where(ok, t, 1.0) / best), 0.0)
+    return y.astype(np.float32), ok.astype(np.float32)
+
+
+def evaluate(choices, times, N):
+    """Regret of chosen classes vs the exhaustive best, next to the default's."""
+    t = np.asarray(times, np.float64)
+    best = np.nanmin(t, axis=1)
+    pick = t[np.arange(len(t)), choices]
+    dflt = np.array([t[i, default_class(int(n))] for i, n in enumerate(N)])
+    reg = pick / best - 1.0
+    dreg = dflt / best - 1.0
+    return dict(n=len(t), regret_mean=float(np.mean(reg)), regret_median=float(np.median(reg)),
+                regret_p90=float(np.quantile(reg, 0.9)), default_regret_mean=float(np.mean(dreg)),
+                speedup_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / pick)))),
+                exhaustive_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / best)))),
+                picked_reorder_frac=float(np.mean([CLASSES[c]["reorder"] for c in choices])))
+
+
+# ------------------------------------------------------- data collection
+FAMILIES = ("rmat", "banded", "blockdiag", "uniform")
+
+
+def sample_spec(rng, nnz_lo, nnz_hi):
+    """One seeded matrix description of the training family."""
+    fam = FAMILIES[int(rng.integers(len(FAMILIES)))]
+    nnz = float(np.exp(rng.uniform(np.log(nnz_lo), np.log(nnz_hi))))
+    spec = dict(family=fam, seed=int(rng.integers(1 << 30)), N=int(rng.choice([128, 512])),
+                shuffle=int(rng.integers(2)))
+    if fam == "rmat":
+        a = float(rng.uniform(0.45, 0.65))
+        rest = 1.0 - a
+        spec.update(a=a, b=rest * 0.19 / 0.43, c=rest * 0.19 / 0.43, edge_factor=8.0,
+                    scale=int(max(10, min(22, round(np.log2(nnz / 8.0 / 2.0))))))
+    elif fam == "banded":
+        bw = int(np.exp(rng.uniform(np.log(8), np.log(512))))
+        fill = float(rng.uniform(0.1, 0.9))
+        spec.update(bandwidth=bw, fill=fill, M=int(max(1024, nnz / max(1.0, 2 * bw * fill))))
+    elif fam == "blockdiag":
+        blk = int(np.exp(rng.uniform(np.log(32), np.log(4096))))
+        deg = int(rng.integers(4, 33))
+        spec.update(block=blk, degree=min(deg, blk), M=int(max(1024, nnz / min(deg, blk))))
+    else:
+        mean = float(np.exp(rng.uniform(np.log(4), np.log(64))))
+        spec.update(mean=mean, M=int(max(1024, nnz / mean)))
+    return spec
+
+
+def make_matrix(spec):
+    f = spec["family"]
+    if f == "rmat":
+        return gen.rmat(spec["scale"], spec["edge_factor"], spec["a"], spec["b"], spec["c"],
+                        seed=spec["seed"])
+    if f == "banded":
+        return gen.banded(spec["M"], spec["bandwidth"], spec["fill"], seed=spec["seed"])
+    if f == "blockdiag":
+        return gen.blockdiag(spec["M"], spec["block"], spec["degree"], 0.05, seed=spec["seed"])
+    return gen.uniform(spec["M"], mean=spec["mean"], seed=spec["seed"])
+
+
+def measure(spec, reps=3, device="cuda"):
+    """Features [48] and the measured kernel time [K] (ms; NaN = infeasible)."""
+    A = make_matrix(spec)
+    N = spec["N"]
+    rp = torch.from_numpy(A.rowptr).to(device)
+    cl = torch.from_numpy(A.col).to(device)
+    vl = torch.from_numpy(A.val).to(device)
+    if spec["shuffle"]:
+        perm = torch.from_numpy(np.random.default_rng(spec["seed"] + 1)
+                                .permutation(A.M).astype(np.int32)).to(device)
+        rp, cl, vl = metcf.permute_csr(rp, cl, vl, perm)
+    m = metcf.convert(rp, cl, A.M, values=vl)
+    feat = features(rp, cl, m, N).cpu().numpy()
+    B = torch.from_numpy(gen.normal(A.M, N, seed=spec["seed"] + 2)).to(device)
+    times = np.full(K, np.nan, np.float32)
+    info = dict(M=A.M, nnz=int(cl.numel()), T0=m.T)
+    for ro in (0, 1):
+        mm = m
+        if ro:
+            t0 = time.perf_counter()
+            _, rp2, c2, v2 = reorder_mod.reorder(rp, cl, vl, A.M)
+            torch.cuda.synchronize()
+            info["tca_s"] = time.perf_counter() - t0
+            mm = metcf.convert(rp2, c2, A.M, values=v2)
+            info["T1"] = mm.T
+        ws = tune.workspace_for(mm, N, B.device)
+        out = torch.empty((A.M, N), dtype=torch.float32, device=device)
+        for fo in FORMS:
+            fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
+            planes = metcf.pack_b(B, fmt)
+            scheds, _ = tune.autotune(mm, planes, fmt, N, prec, reps=reps, out=out, workspace=ws)
+            for s in scheds:
+                times[class_of(s.mode, s.waves, s.ntile, fo, ro)] = s.ms
+        del ws, out
+    return feat, times, info
+
+
+def collect(n_train, n_test, seed=0, nnz_lo=2 ** 18, nnz_hi=2 ** 22, reps=3, log=None):
+    """Measured dataset over seeded synthetic matrices (train, then held-out)."""
+    rng = np.random.default_rng(seed)
+    specs = [sample_spec(rng, nnz_lo, nnz_hi) for _ in range(n_train + n_test)]
+    F, Tm, meta = [], [], []
+    for i, sp in enumerate(specs):
+        t0 = time.perf_counter()
+        f, t, info = measure(sp, reps=reps)
+        F.append(f)
+        Tm.append(t)
+        meta.append(dict(sp, **info, split="train" if i < n_train else "test"))
+        if log:
+            log(f"[{i + 1}/{len(specs)}] {sp['family']} N={sp['N']} nnz={info['nnz']} "
+                f"best={np.nanmin(t):.3f}ms {time.perf_counter() - t0:.1f}s")
+    return dict(features=np.stack(F), times=np.stack(Tm), meta=meta)
+
+
+def save_dataset(ds, path=DATASET_PATH):
+    import json
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez_compressed(path, features=ds["features"], times=ds["times"],
+                        meta=np.array(json.dumps(ds["meta"])))
+
+
+def load_dataset(path=DATASET_PATH):
+    import json
+    z = np.load(path)
+    return dict(features=z["features"], times=z["times"], meta=json.loads(str(z["meta"])))
+
+
+def split(ds):
+    tr = np.array([m["split"] == "train" for m in ds["meta"]])
+    N = np.array([m["N"] for m in ds["meta"]])
+    return tr, N
+
+
+def fit(ds, steps=3000, lr=2e-3, seed=0, device="cuda"):
+    """Trains on the dataset's train split; returns (model, held-out evaluation)."""
+    tr, N = split(ds)
+    y, mk = targets(ds["times"])
+    net = MLP(seed=seed, device=device)
+    net.train(ds["features"][tr], y[tr], mk[tr], steps=steps, lr=lr, seed=seed)
+    feas = np.stack([feasible(int(n)) for n in N[~tr]])
+    ch = net.choose(ds["features"][~tr], feas)
+    return net, evaluate(ch, ds["times"][~tr], N[~tr])
+
+
+# ------------------------------------------------------------- scheduler
+@dataclass
+class Plan:
+    cls: int
+    form: str
+    reorder: bool
+    mode: int
+    waves: int
+    ntile: int
+    source: str  # "model" or "exhaustive"
+
+
+class Scheduler:
+    """Picks a class for (matrix, N): the trained model when its weights are
+    present, else the exhaustive autotuner over every class."""
+
+    def __init__(self, weights=WEIGHTS_PATH, device="cuda"):
+        self.net = MLP.load(weights, device) if weights and os.path.exists(weights) else None
+
+    def plan(self, rowptr, col, m: metcf.METCF, N, exhaustive=False, B=None, reps=3):
+        if self.net is not None and not exhaustive:
+            f = features(rowptr, col, m, N).reshape(1, -1)
+            c = int(self.net.choose(f, feasible(N))[0])
+            src = "model"
+        else:
+            c = self._exhaustive(rowptr, col, m, N, B, reps)
+            src = "exhaustive"
+        k = CLASSES[c]
+        return Plan(c, k["form"], bool(k["reorder"]), k["mode"], k["waves"], k["ntile"], src)
+
+    @staticmethod
+    def _exhaustive(rowptr, col, m, N, B, reps):
+        dev = m.RowWindowOffset.device
+        if B is None:
+            B = torch.randn((m.M, N), device=dev)
+        best, best_c = None, None
+        for ro in (0, 1):
+            mm = m
+            if ro:
+                _, rp2, c2, v2 = reorder_mod.reorder(rowptr.to(dev), col.to(dev), None, m.M)
+                mm = metcf.convert(rp2, c2, m.M, values=v2)
+            for fo in FORMS:
+                fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
+                scheds, b = tune.autotune(mm, metcf.pack_b(B, fmt), fmt, N, prec, reps=reps)
+                if best is None or b.ms < best:
+                    best, best_c = b.ms, class_of(b.mode, b.waves, b.ntile, fo, ro)
+        return best_c
+
+
+def main(argv=None):
+    """python -m dtc_b200.costmodel collect|train ... (dataset + weights under data/)."""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cmd", choices=["collect", "train"])
+    ap.add_argument("--train", type=int, default=400)
+    ap.add_argument("--test", type=int, default=100)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--nnz-lo", type=float, default=2 ** 18)
+    ap.add_argument("--nnz-hi", type=float, default=2 ** 22)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--dataset", default=DATASET_PATH)
+    ap.add_argument("--weights", default=WEIGHTS_PATH)
+    a = ap.parse_args(argv)
+    if a.cmd == "collect":
+        ds = collect(a.train, a.test, a.seed, a.nnz_lo, a.nnz_hi, a.reps, log=print)
+        save_dataset(ds, a.dataset)
+    ds = load_dataset(a.dataset)
+    net, ev = fit(ds, steps=a.steps, seed=a.seed)
+    net.save(a.weights, eval=np.array(str(ev)))
+    print(ev)
+
+
+if __name__ == "__main__":
+    main()

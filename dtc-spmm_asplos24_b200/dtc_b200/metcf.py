@@ -165,6 +165,35 @@ def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True
     return C_
 
 
+def spmm_fused(m: METCF, planes, fmt, N, precision, bias=None, relu=False, mode=0, grid=0,
+               ntile=0, use_values=True, out=None, workspace=None):
+    """spmm_ex with C = act(A*B + bias) fused into the store of C (GCN epilogue)."""
+    dev = planes[0].device
+    C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
+    wsb = C.c_size_t()
+    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, mode, grid, C.byref(wsb))
+    ws = workspace
+    if ws is None and wsb.value:
+        ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
+    vals = m.TCvalues if use_values else None
+    bias = None if bias is None else bias.to(torch.float32).contiguous()
+    call("dtc_spmm_fused", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId),
+         _ptr(m.TCblockoffset), _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, fmt,
+         _ptr(planes[0]), _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(bias),
+         1 if relu else 0, _ptr(C_), mode, grid, ntile, _ptr(ws), 0 if ws is None else ws.numel(),
+         _stream())
+    return C_
+
+
+def gcn_layer(m: METCF, H, W, bias=None, relu=True, fmt=0, precision=0, mode=0, grid=0):
+    """One GCN layer act(Â (H W) + b): the dense H W on cuBLAS, then the SpMM with
+    bias + ReLU fused into its epilogue (one pass over C instead of two)."""
+    XW = torch.mm(H, W).contiguous()
+    N = XW.shape[1]
+    planes = [XW] if fmt == 0 else pack_b(XW, fmt)
+    return spmm_fused(m, planes, fmt, N, precision, bias=bias, relu=relu, mode=mode, grid=grid)
+
+
 def _relabel(name, rowptr, col, val, rows_out, extra):
     dev = rowptr.device
     rows_in = rowptr.numel() - 1

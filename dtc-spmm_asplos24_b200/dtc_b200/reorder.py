@@ -1,0 +1,39 @@
+"""Row reordering: the TCA clustering permutation (dtc_tca_reorder) and its
+application (dtc_permute_csr), the GPU form of reordering/TCA_reorder.py and
+the CSR rebuild of scripts/DTCSpMM/dataset.py:38-44."""
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import TcaParams, call
+from .metcf import _ptr, _stream, permute_csr
+
+
+def default_params(**overrides):
+    p = TcaParams()
+    _lib.lib().dtc_tca_default_params(C.byref(p))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def tca_perm(rowptr, col, num_nodes, params=None):
+    """perm[new] = old (int32 device tensor) for a square CSR on the device."""
+    rowptr = rowptr.to(torch.int32).contiguous()
+    col = col.to(torch.int32).contiguous()
+    p = params if params is not None else default_params()
+    b = C.c_size_t()
+    call("dtc_tca_workspace_bytes", num_nodes, col.numel(), C.byref(p), C.byref(b))
+    ws = torch.empty(max(b.value, 1), dtype=torch.uint8, device=rowptr.device)
+    perm = torch.empty(max(num_nodes, 1), dtype=torch.int32, device=rowptr.device)
+    call("dtc_tca_reorder", _ptr(rowptr), _ptr(col), num_nodes, col.numel(), C.byref(p),
+         _ptr(perm), _ptr(ws), ws.numel(), _stream())
+    return perm[:num_nodes]
+
+
+def reorder(rowptr, col, val, num_nodes, params=None):
+    """(perm, rowptr', col', val') with A' = P A Pᵀ under the TCA permutation."""
+    perm = tca_perm(rowptr, col, num_nodes, params)
+    rp, c, v = permute_csr(rowptr, col, val, perm)
+    return perm, rp, c, v

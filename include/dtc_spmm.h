@@ -110,6 +110,39 @@ dtc_status dtc_transpose_csr(const int32_t* d_rowptr, const int32_t* d_col, cons
                              int64_t* nnz_out, void* d_workspace, size_t workspace_bytes,
                              dtc_stream_t stream);
 
+/* TCA reorder: two-level MinHash-LSH + Jaccard greedy clustering of rows
+ * (reordering/TCA_reorder.py:53-326; its MinHash/LSH come from datasketch and
+ * cuGraph, absent here, so hashing and banding are this library's own).
+ * Writes d_perm[num_nodes] (d_perm[new] = old) for dtc_permute_csr. Row sets
+ * are the distinct columns of each row of a square CSR matrix. Synchronises
+ * `stream`; the merge loop runs on the host. Deterministic for given params. */
+typedef struct {
+  int32_t num_perm;       /* MinHash functions (reference: 128)                  */
+  int32_t bands;          /* LSH bands; bands * rows_per_band <= num_perm        */
+  int32_t rows_per_band;  /* (42 x 3 puts the LSH threshold near 0.2-0.3)        */
+  int32_t thres;          /* level-1 cluster size cap in rows (reference: 16)    */
+  int32_t c_thres;        /* level-2 cap in clusters (reference: 128)            */
+  int32_t bucket_window;  /* each item pairs with this many bucket successors    */
+  uint64_t seed;
+} dtc_tca_params;
+
+void dtc_tca_default_params(dtc_tca_params* params);
+dtc_status dtc_tca_workspace_bytes(int32_t num_nodes, int64_t nnz, const dtc_tca_params* params,
+                                   size_t* bytes);
+dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_t num_nodes,
+                           int64_t nnz, const dtc_tca_params* params, int32_t* d_perm,
+                           void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+
+/* COO edge list -> canonical CSR: the CSR build of the reference's loader
+ * (scripts/DTCSpMM/dataset.py:21-44: src_li / dst_li / num_nodes of an .npz,
+ * coo_matrix((1, (src, dst))).tocsr()). d_val == NULL gives every edge the
+ * value 1, so duplicate edges sum to their multiplicity like the reference's.
+ * Output arrays hold num_rows+1 / nnz entries. */
+dtc_status dtc_coo_to_csr(const int32_t* d_src, const int32_t* d_dst, const float* d_val,
+                          int32_t num_rows, int32_t num_cols, int64_t nnz, int32_t* d_rowptr_out,
+                          int32_t* d_col_out, float* d_val_out, int64_t* nnz_out,
+                          void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+
 /* ------------------------------------------------------------------------- */
 /* Dense-operand storage forms ("B formats").                                  */
 /* ------------------------------------------------------------------------- */
@@ -202,6 +235,18 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
 dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
                                        int grid, size_t* bytes);
 
+/* dtc_spmm_ex with the GCN layer's epilogue fused into the store of C:
+ * C = act(A*B + bias), bias[N] per column (NULL = none), act = ReLU when
+ * relu != 0. Replaces DTCSpMM_gcn (DTC-SpMM/DTCSpMM.cpp:147-161 ->
+ * DTCSpMM_kernel.cu:1033-1116) followed by a separate bias/activation pass. */
+dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
+                          const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
+                          const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
+                          int64_t num_blocks, int bformat, const void* d_Bplane0,
+                          const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
+                          int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
+                          size_t workspace_bytes, dtc_stream_t stream);
+
 /* ------------------------------------------------------------------------- */
 /* Schedule autotuner. Replaces the reference's hand-written schedule table   */
 /* (scripts/DTCSpMM/run_DTC_SpMM.py:10-30: balance yes/no, vector width and   */
@@ -237,6 +282,59 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
                         void* d_workspace, size_t workspace_bytes, int reps,
                         dtc_schedule* results, int max_results, int* num_results, int* best,
                         dtc_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Learned schedule cost model (no reference counterpart: the reference's     */
+/* schedule is the fixed table of scripts/DTCSpMM/run_DTC_SpMM.py:10-30).      */
+/* ------------------------------------------------------------------------- */
+
+/* 48 structural features of a square CSR matrix and its ME-TCF form (row-length
+ * histogram, TC blocks per window, nonzeros per block, column locality, sizes;
+ * the layout is listed in the library's features source) into d_features[48].
+ * Needs the ME-TCF row-window offsets, block offsets and edgeToColumn (the
+ * conversion's in-place output). Bitwise reproducible. */
+size_t dtc_features_workspace_bytes(void);
+dtc_status dtc_features(const int32_t* d_rowptr, const int32_t* d_col, int32_t num_nodes,
+                        int64_t nnz, const int32_t* d_rowWindowOffset,
+                        const int32_t* d_tcblockOffset, const int32_t* d_edgeToColumn,
+                        int32_t num_windows, int64_t num_blocks, int32_t N, float* d_features,
+                        void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
+
+/* MLP in -> h1 -> h2 -> out, ReLU hidden layers, linear output. Parameters are
+ * one fp32 vector: W1[h1][in], b1[h1], W2[h2][h1], b2[h2], W3[out][h2], b3[out];
+ * activations are row-major [batch][width]. */
+typedef struct {
+  int32_t in, h1, h2, out;
+} dtc_mlp_dims;
+
+/* Number of parameters, or -1 for invalid dims (each in [1, 4096]). */
+int64_t dtc_mlp_num_params(const dtc_mlp_dims* dims);
+
+/* Forward pass: d_H1[batch][h1], d_H2[batch][h2] (post-ReLU), d_Y[batch][out]. */
+dtc_status dtc_mlp_forward(const dtc_mlp_dims* dims, const float* d_params, const float* d_X,
+                           int32_t batch, float* d_H1, float* d_H2, float* d_Y,
+                           dtc_stream_t stream);
+
+/* Masked MSE loss L = sum mask*(Y-target)^2 / sum mask into *d_loss and its
+ * gradient with respect to every parameter into d_grads (same layout as the
+ * parameters), from the activations of dtc_mlp_forward. Deterministic. */
+size_t dtc_mlp_backward_workspace_bytes(const dtc_mlp_dims* dims, int32_t batch);
+dtc_status dtc_mlp_backward(const dtc_mlp_dims* dims, const float* d_params, const float* d_X,
+                            const float* d_H1, const float* d_H2, const float* d_Y,
+                            const float* d_target, const float* d_mask, int32_t batch,
+                            float* d_grads, float* d_loss, void* d_workspace,
+                            size_t workspace_bytes, dtc_stream_t stream);
+
+/* One Adam step (bias-corrected, step >= 1) over n parameters. */
+dtc_status dtc_mlp_adam(float* d_params, const float* d_grads, float* d_m, float* d_v, int64_t n,
+                        float lr, float beta1, float beta2, float eps, int32_t step,
+                        dtc_stream_t stream);
+
+/* d_choice[r] = argmin over feasible outputs of d_Y[r][.] (lowest index on
+ * ties, -1 if none is feasible). d_feasible: NULL (all), one row shared by all
+ * (feasible_per_row = 0) or one row per input (feasible_per_row = 1). */
+dtc_status dtc_mlp_argmin(const float* d_Y, const uint8_t* d_feasible, int feasible_per_row,
+                          int32_t batch, int32_t out, int32_t* d_choice, dtc_stream_t stream);
 
 /* d_rowWindowOffset[num_windows+1] from a sorted d_tcblockRowid[T]. */
 dtc_status dtc_rowid_to_window_offset(const int32_t* d_tcblockRowid, int64_t num_blocks,

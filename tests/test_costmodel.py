@@ -1,0 +1,171 @@
+"""Learned schedule cost model.
+
+CPU: the oracle's hand-written chain rule is pinned by finite differences; the
+class space, targets and regret arithmetic are checked on fixed numbers; the
+committed measured dataset is well formed.
+GPU: dtc_features equals the oracle's features; the MLP forward, backward
+(gradients) and Adam kernels match the FP64 oracle; training is bitwise
+reproducible; and on the committed dataset's held-out matrices the trained
+network beats the untuned default schedule and has lower regret against the
+exhaustive autotuner.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import costmodel_oracle as CO
+from dtc_b200 import costmodel as cm
+
+DIMS = (48, 64, 64, cm.K)
+
+
+def _rand_params(dims, seed=0, scale=0.3):
+    n = sum(a * b + b for a, b in zip(dims[:-1], dims[1:]))
+    return np.random.default_rng(seed).standard_normal(n).astype(np.float32) * scale
+
+
+def test_oracle_gradients_match_finite_differences():
+    dims = (5, 7, 6, 4)
+    p = _rand_params(dims, 1).astype(np.float64)
+    rng = np.random.default_rng(2)
+    X = rng.standard_normal((9, 5))
+    T = rng.standard_normal((9, 4))
+    Mk = (rng.random((9, 4)) < 0.7).astype(np.float64)
+    _, g = CO.loss_and_grads(p, dims, X, T, Mk)
+    h = 1e-6
+    for i in rng.choice(len(p), 25, replace=False):
+        e = np.zeros_like(p)
+        e[i] = h
+        fd = (CO.loss_and_grads(p + e, dims, X, T, Mk)[0] -
+              CO.loss_and_grads(p - e, dims, X, T, Mk)[0]) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
+
+
+def test_class_space():
+    assert cm.K == 2 * 2 * 2 * 5 * 3
+    assert cm.feasible(128).sum() == cm.K // 3
+    assert cm.feasible(512).sum() == cm.K
+    d = cm.CLASSES[cm.default_class(512)]
+    assert (d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == (1, 16, 4, "split24x4", 0)
+    assert all(c["H"] == 16 and c["W"] == 8 for c in cm.CLASSES)
+
+
+def test_targets_and_regret():
+    t = np.full((2, cm.K), np.nan, np.float32)
+    t[0, :4] = [2.0, 1.0, 4.0, 1.5]
+    t[1, :] = 3.0
+    t[1, cm.default_class(128)] = 6.0
+    y, mk = cm.targets(t)
+    assert mk[0].sum() == 4 and mk[1].sum() == cm.K
+    np.testing.assert_allclose(y[0, :4], np.log([2.0, 1.0, 4.0, 1.5]), rtol=1e-6)
+    t[0, cm.default_class(128)] = 2.0
+    ev = cm.evaluate(np.array([1, 0]), t, np.array([128, 128]))
+    assert ev["regret_mean"] == pytest.approx(0.0)
+    assert ev["default_regret_mean"] == pytest.approx((1.0 + 1.0) / 2)
+    assert ev["speedup_vs_default_geomean"] == pytest.approx(2.0)
+
+
+def test_committed_dataset_well_formed():
+    if not os.path.exists(cm.DATASET_PATH):
+        pytest.skip("no measured dataset committed")
+    ds = cm.load_dataset()
+    S = len(ds["meta"])
+    assert ds["features"].shape == (S, 48) and ds["times"].shape == (S, cm.K)
+    tr, N = cm.split(ds)
+    assert tr.sum() > 0 and (~tr).sum() > 0
+    for i in range(S):
+        f = cm.feasible(int(N[i])).astype(bool)
+        assert np.isfinite(ds["times"][i][f]).all() and np.isnan(ds["times"][i][~f]).all()
+    assert {m["family"] for m in ds["meta"]} == set(cm.FAMILIES)
+
+
+# ------------------------------------------------------------------ GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small_uniform", "hub", "empty_windows", "banded_dense"])
+def test_features_match_oracle(cuda, name):
+    import torch
+    from oracle import oracle as O
+    from dtc_b200 import metcf
+    from tests.golden import cases
+    rp, col, val, M = cases.CASES[name]()
+    m = metcf.convert(rp, col, M)
+    got = cm.features(torch.from_numpy(rp), torch.from_numpy(col), m, 128).cpu().numpy()
+    ref = CO.features(rp, col, M, O.metcf(rp, col, M), 128)
+    logs = [36, 37, 38, 39, 40, 41]
+    exact = [i for i in range(48) if i not in logs]
+    np.testing.assert_array_equal(got[exact], ref[exact])
+    np.testing.assert_allclose(got[logs], ref[logs], rtol=1e-6)
+
+
+@pytest.mark.gpu
+def test_mlp_forward_backward_adam_match_oracle(cuda):
+    import torch
+    rng = np.random.default_rng(3)
+    p = _rand_params(DIMS, 4, scale=0.2)
+    net = cm.MLP(DIMS, params=p)
+    B = 37
+    X = rng.random((B, 48)).astype(np.float32)
+    T = rng.standard_normal((B, cm.K)).astype(np.float32)
+    Mk = (rng.random((B, cm.K)) < 0.5).astype(np.float32)
+    H1, H2, Y = (t.cpu().numpy() for t in net.forward(X))
+    rH1, rH2, rY = CO.forward(p, DIMS, X)
+    np.testing.assert_allclose(Y, rY, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(H2, rH2, rtol=1e-5, atol=1e-5)
+    loss, g = net.loss_and_grads(X, T, Mk)
+    rl, rg = CO.loss_and_grads(p, DIMS, X, T, Mk)
+    assert float(loss.item()) == pytest.approx(rl, rel=1e-5)
+    g = g.cpu().numpy()
+    np.testing.assert_allclose(g, rg, rtol=1e-4, atol=1e-5 * np.abs(rg).max())
+    m0 = torch.zeros(net.n, device="cuda")
+    v0 = torch.zeros(net.n, device="cuda")
+    gd = torch.from_numpy(rg.astype(np.float32)).cuda()
+    from dtc_b200._lib import call
+    from dtc_b200.metcf import _ptr, _stream
+    for step in (1, 2):
+        call("dtc_mlp_adam", _ptr(net.params), _ptr(gd), _ptr(m0), _ptr(v0), net.n, 1e-3, 0.9,
+             0.999, 1e-8, step, _stream())
+    rp_, rm, rv = CO.adam(p, rg.astype(np.float32), np.zeros(net.n), np.zeros(net.n), 1e-3, 0.9,
+                          0.999, 1e-8, 1)
+    rp_, rm, rv = CO.adam(rp_, rg.astype(np.float32), rm, rv, 1e-3, 0.9, 0.999, 1e-8, 2)
+    np.testing.assert_allclose(net.params.cpu().numpy(), rp_, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.gpu
+def test_argmin_respects_feasibility(cuda):
+    net = cm.MLP(DIMS, params=_rand_params(DIMS, 5))
+    X = np.random.default_rng(6).random((8, 48)).astype(np.float32)
+    _, _, Y = net.forward(X)
+    Y = Y.cpu().numpy()
+    feas = cm.feasible(128)
+    ch = net.choose(X, feas)
+    for r in range(8):
+        ok = np.flatnonzero(feas)
+        assert ch[r] == ok[np.argmin(Y[r, ok])]
+
+
+@pytest.mark.gpu
+def test_training_reproducible_and_descends(cuda):
+    rng = np.random.default_rng(7)
+    X = rng.random((64, 48)).astype(np.float32)
+    T = rng.random((64, cm.K)).astype(np.float32)
+    Mk = np.ones_like(T)
+    a = cm.MLP(DIMS, seed=1)
+    b = cm.MLP(DIMS, seed=1)
+    ha = a.train(X, T, Mk, steps=200, log_every=50)
+    b.train(X, T, Mk, steps=200)
+    assert np.array_equal(a.params.cpu().numpy().view(np.uint32),
+                          b.params.cpu().numpy().view(np.uint32))
+    assert ha[-1][1] < 0.5 * ha[0][1]
+
+
+@pytest.mark.gpu
+def test_trained_model_beats_default_on_held_out(cuda):
+    """What the network gains over the method without it, on held-out matrices."""
+    if not os.path.exists(cm.DATASET_PATH):
+        pytest.skip("no measured dataset committed")
+    ds = cm.load_dataset()
+    net, ev = cm.fit(ds, steps=2000, seed=0)
+    assert ev["speedup_vs_default_geomean"] > 1.0, ev
+    assert ev["regret_mean"] < ev["default_regret_mean"], ev
+    assert ev["regret_median"] < 0.10, ev

@@ -168,3 +168,42 @@ def test_extension_api_matches_c_abi(cuda):
 def test_no_device_errors_recorded(cuda):
     from dtc_b200 import metcf
     assert metcf.device_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("form", ["tf32", "split24x4"])
+@pytest.mark.parametrize("name", ["hub", "empty_windows", "small_uniform"])
+def test_fused_bias_relu_epilogue(cuda, name, form, mode):
+    """C = ReLU(A B + bias) from one launch, windows split across CTAs included."""
+    import torch
+    from dtc_b200 import metcf, tune
+    rp, col, val, M = cases.CASES[name]()
+    m = metcf.convert(rp, col, M, values=val)
+    N = 64
+    B = np.random.default_rng(11).standard_normal((M, N)).astype(np.float32)
+    bias = np.random.default_rng(12).standard_normal(N).astype(np.float32)
+    fmt, prec = tune.FORMS[form][0], tune.FORMS[form][1]
+    Bd = torch.from_numpy(B).cuda()
+    planes = [Bd] if form == "tf32" else metcf.pack_b(Bd, fmt)
+    C = metcf.spmm_fused(m, planes, fmt, N, prec, bias=torch.from_numpy(bias).cuda(), relu=True,
+                         mode=mode, grid=7 if mode else 0).cpu().numpy().astype(np.float64)
+    ref = np.maximum(O.spmm_f64(rp, col, val, M, B) + bias, 0.0)
+    bound = O.spmm_absbound_f64(rp, col, val, M, B)
+    tol = 2.0 ** -9 if form == "tf32" else 2.0 ** -14
+    assert (np.abs(C - ref) <= tol * bound + 1e-6).all()
+    assert metcf.device_status(clear=True) == 0
+
+
+def test_gcn_entry_bias_relu(cuda):
+    import torch
+    import DTCSpMM
+    from dtc_b200 import metcf
+    rp, col, _, M = cases.small_uniform()
+    m = metcf.convert(rp, col, M)
+    X = torch.randn(M, 32, device="cuda")
+    b = torch.randn(32, device="cuda")
+    (C,) = DTCSpMM.DTCSpMM_gcn(X, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                               m.SparseAToX, M, len(col), bias=b, relu=True)
+    (P,) = DTCSpMM.DTCSpMM_gcn(X, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
+                               m.SparseAToX, M, len(col))
+    torch.testing.assert_close(C, torch.relu(P + b), rtol=0, atol=1e-6)

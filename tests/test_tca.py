@@ -1,0 +1,77 @@
+"""TCA reorder (reordering/TCA_reorder.py:53-326): the library's permutation is
+bit-exact with the oracle's restatement (same hashing, banding and merge
+rules), is a permutation, respects the level-1 cluster cap, and reduces the
+ME-TCF block count on a matrix with hidden row clusters."""
+import numpy as np
+import pytest
+
+from oracle import tca_oracle as TO
+
+
+def clustered(M=480, groups=30, seed=0):
+    """Rows in hidden groups sharing column sets, shuffled over the row ids."""
+    rng = np.random.default_rng(seed)
+    pool = [rng.choice(M, 12, replace=False) for _ in range(groups)]
+    owner = rng.permutation(np.arange(M) % groups)
+    rows = []
+    for i in range(M):
+        base = pool[owner[i]]
+        keep = base[rng.random(len(base)) < 0.85]
+        extra = rng.choice(M, 1)
+        rows.append(np.unique(np.concatenate([keep, extra])))
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    return rp, np.concatenate(rows).astype(np.int32), M
+
+
+def test_oracle_clusters_respect_caps():
+    rp, col, M = clustered(M=200, groups=10)
+    perm = TO.tca_perm(rp, col, M, thres=16)
+    assert sorted(perm.tolist()) == list(range(M))
+    rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(M)]
+    sig = TO.signatures(rows, 128, 2022)
+    roots = TO.greedy_merge(rows, TO.lsh_pairs(sig, 42, 3, 8), 16)
+    sizes = np.bincount(roots)
+    # a cluster stops growing once it reaches the cap; the last merge can overshoot
+    assert sizes.max() < 2 * 16
+
+
+def test_oracle_mix64_matches_vectorised():
+    xs = [0, 1, 2 ** 63 + 5, 123456789]
+    np.testing.assert_array_equal(TO._mix64_np(np.array(xs, np.uint64)),
+                                  np.array([TO._mix64(x) for x in xs], np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1])
+def test_tca_perm_bit_exact(cuda, seed):
+    import torch
+    from dtc_b200 import reorder
+    rp, col, M = clustered(seed=seed)
+    got = reorder.tca_perm(torch.from_numpy(rp).cuda(), torch.from_numpy(col).cuda(), M)
+    ref = TO.tca_perm(rp, col, M)
+    np.testing.assert_array_equal(got.cpu().numpy(), ref)
+
+
+@pytest.mark.gpu
+def test_tca_perm_with_empty_rows_and_hub(cuda):
+    import torch
+    from dtc_b200 import reorder
+    from tests.golden import cases
+    rp, col, _, M = cases.hub()
+    got = reorder.tca_perm(torch.from_numpy(rp).cuda(), torch.from_numpy(col).cuda(), M,
+                           reorder.default_params(thres=8, c_thres=16))
+    ref = TO.tca_perm(rp, col, M, thres=8, c_thres=16)
+    np.testing.assert_array_equal(got.cpu().numpy(), ref)
+
+
+@pytest.mark.gpu
+def test_tca_reduces_blocks_on_hidden_clusters(cuda):
+    import torch
+    from dtc_b200 import metcf, reorder
+    rp, col, M = clustered(M=2048, groups=128, seed=3)
+    rpd, cd = torch.from_numpy(rp).cuda(), torch.from_numpy(col).cuda()
+    T0 = metcf.convert(rpd, cd, M).T
+    perm, rp2, c2, _ = reorder.reorder(rpd, cd, None, M)
+    T1 = metcf.convert(rp2, c2, M).T
+    assert sorted(perm.cpu().tolist()) == list(range(M))
+    assert T1 < 0.8 * T0, (T0, T1)
