@@ -148,11 +148,12 @@ dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tile
                         nwin, num_blocks, d_B, N, d_C, 1, 0, part, st);
 }
 
-dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
-                                       int grid, size_t* bytes) {
+dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                       int32_t block_h, int mode, int grid, size_t* bytes) {
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
-  *bytes = (mode == 1) ? spmm_partials_bytes(num_blocks, N, grid) : 0;
+  DTC_REQUIRE(block_h == 16 || block_h == 32, "block_h must be 16 or 32");
+  *bytes = (mode == 1) ? spmm_partials_bytes(num_blocks, N, grid, block_h) : 0;
   return DTC_OK;
 }
 
@@ -162,15 +163,15 @@ namespace {
 
 dtc_status spmm_ex_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                         const int32_t* s2x, const float* vals, int32_t M, int32_t nwin, int64_t T,
-                        int bformat, const void* p0, const void* p1, int32_t N, int precision,
-                        float* C, int mode, int grid, int ntile, Epilogue epi, void* ws,
-                        size_t wsb, cudaStream_t st) {
+                        int32_t H, int bformat, const void* p0, const void* p1, int32_t N,
+                        int precision, float* C, int mode, int grid, int ntile, Epilogue epi,
+                        void* ws, size_t wsb, cudaStream_t st) {
   DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
   DTC_REQUIRE(grid >= 0, "grid must be >= 0");
   DTC_REQUIRE(ntile == 0 || ntile == 1 || ntile == 2 || ntile == 4, "ntile must be 0, 1, 2 or 4");
   DTC_REQUIRE(rwo && toff && p0 && C, "null device pointer");
   size_t need = 0;
-  dtc_status s = dtc_spmm_ex_workspace_bytes(M, T, N, mode, grid, &need);
+  dtc_status s = dtc_spmm_ex_workspace_bytes(M, T, N, H, mode, grid, &need);
   if (s != DTC_OK) return s;
   if (need > 0 && (!ws || wsb < need)) {
     set_error("spmm workspace too small");
@@ -178,9 +179,9 @@ dtc_status spmm_ex_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* 
   }
   if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
     return spmm_tf32_impl(rwo, tile, toff, s2x, vals, M, nwin, T, (const float*)p0, N, C, mode,
-                          grid, (float*)ws, st, ntile, epi);
+                          grid, (float*)ws, st, ntile, epi, H);
   return spmm_split_impl(rwo, tile, toff, s2x, vals, M, nwin, T, bformat, p0, p1, N, precision,
-                         C, mode, grid, (float*)ws, st, ntile, epi);
+                         C, mode, grid, (float*)ws, st, ntile, epi, H);
 }
 
 }  // namespace
@@ -190,12 +191,12 @@ extern "C" {
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                       int64_t num_blocks, int bformat, const void* d_Bplane0,
+                       int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                        const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
                        int grid, int ntile, void* d_workspace, size_t workspace_bytes,
                        dtc_stream_t stream) {
   return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
-                      num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
+                      num_nodes, num_windows, num_blocks, block_h, bformat, d_Bplane0, d_Bplane1, N,
                       precision, d_C, mode, grid, ntile, Epilogue{}, d_workspace,
                       workspace_bytes, (cudaStream_t)stream);
 }
@@ -203,7 +204,7 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
 dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                           const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                           const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                          int64_t num_blocks, int bformat, const void* d_Bplane0,
+                          int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                           const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
                           int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
                           size_t workspace_bytes, dtc_stream_t stream) {
@@ -211,8 +212,8 @@ dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_til
   e.bias = d_bias;
   e.relu = relu != 0;
   return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
-                      num_nodes, num_windows, num_blocks, bformat, d_Bplane0, d_Bplane1, N,
-                      precision, d_C, mode, grid, ntile, e, d_workspace, workspace_bytes,
+                      num_nodes, num_windows, num_blocks, block_h, bformat, d_Bplane0, d_Bplane1,
+                      N, precision, d_C, mode, grid, ntile, e, d_workspace, workspace_bytes,
                       (cudaStream_t)stream);
 }
 

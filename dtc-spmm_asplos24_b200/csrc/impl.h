@@ -15,13 +15,14 @@ struct Epilogue {
 dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile = 0, Epilogue epi = {});
+                          float* part, cudaStream_t st, int ntile = 0, Epilogue epi = {},
+                          int H = 16);
 dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile = 0, Epilogue epi = {});
-size_t spmm_partials_bytes(int64_t T, int32_t N, int grid);
+                           cudaStream_t st, int ntile = 0, Epilogue epi = {}, int H = 16);
+size_t spmm_partials_bytes(int64_t T, int32_t N, int grid, int H = 16);
 dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
                         cudaStream_t st);
 dtc_status spmm_mma_sync_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,

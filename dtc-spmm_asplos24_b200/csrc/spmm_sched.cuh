@@ -7,7 +7,6 @@
 namespace dtc {
 namespace {
 
-constexpr int kWinH = 16;       // row-window height (BLK_H)
 // Default CTA count: the kernels hold one CTA per SM (shared memory), so 16
 // CTAs per SM run as 16 waves; a CTA that finishes early picks up the next
 // range, which evens out the per-range cost differences of skewed matrices.
@@ -30,6 +29,7 @@ struct Params {
   const float* bias;         // epilogue bias [N] or null
   int32_t relu;              // epilogue ReLU
   int32_t M, nwin, N, G, mode;
+  int32_t H;                 // row-window height (16 or 32)
   int64_t T;
 };
 
@@ -113,8 +113,8 @@ __global__ void k_reduce_partials(const Params p) {
   // contributors: CTA c-1 (tail slot), CTAs c..c_last (head slots)
   int c_last = c;
   while (c_last + 1 < p.G && (int64_t)(c_last + 1) * p.T / p.G < r1) ++c_last;
-  const int64_t row0 = (int64_t)w * kWinH;
-  const int64_t elems = (int64_t)kWinH * p.N;
+  const int64_t row0 = (int64_t)w * p.H;
+  const int64_t elems = (int64_t)p.H * p.N;
   for (int64_t x = threadIdx.x; x < elems; x += blockDim.x) {
     const int r = (int)(x / p.N);
     if (row0 + r >= p.M) continue;

@@ -47,26 +47,30 @@ constexpr int kConvWarp0 = kTileWarp0 + kTileWarps;  // warps 16-23
 constexpr int kConvWarps = 8;
 constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 768
 constexpr int kTileBytes = 4096;  // per block and 128-feature tile: 16 K rows x 128 bf16
-constexpr int kYBytes = 1024;     // 16 K x 32 N bf16, K-major core matrices
 
 enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2 };
 
-template <int FORM, int NT, int P, int S>
+// WH = row-window height; the UMMA N dimension is 2 WH (A_hi^T | A_lo^T).
+template <int FORM, int NT, int P, int S, int WH>
 struct SCfg {
   static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kMmaWarps == 0 &&
                     S % kConvWarps == 0, "ownership");
   static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
-  static constexpr int kNacc = (NT == 4) ? 2 : 4;
+  static_assert(WH == 16 || WH == 32, "window height");
+  static_assert(NT * WH <= 64, "TMEM budget: two accumulator sets per issuer");
+  static constexpr int kAccCols = NT * 2 * WH;  // TMEM columns of one accumulator set
+  static constexpr int kNacc = 512 / (kMmaWarps * kAccCols) < 4 ? 512 / (kMmaWarps * kAccCols) : 4;
+  static constexpr int kYB = 64 * WH;  // 16 K x 2WH N bf16, K-major core matrices
   static constexpr int kStageX = P * NT * kTileBytes;
   static constexpr int kRowStage = NT * 128;  // staged bytes of one gathered row (u8 / e4m3)
   static constexpr int kStageE = (FORM == kFormBF16) ? 0 : P * kBlkW * kRowStage;
-  static constexpr int kStageY = P * kYBytes;
+  static constexpr int kStageY = P * kYB;
   static constexpr int kX = S * kStageX;
   static constexpr int kE = S * kStageE;
   static constexpr int kY = S * kStageY;
   static constexpr int kBars = (3 * S + 2 * kNacc) * 8;
   static constexpr int kSmem = kX + kE + kY + kBars + 16 + 1024;
-  static constexpr int kCols = kMmaWarps * kNacc * NT * 32;
+  static constexpr int kCols = kMmaWarps * kNacc * kAccCols;
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
                                         : kCols <= 256 ? 256 : 512;
@@ -91,9 +95,9 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
 
-template <int FORM, int NT, int P, int S, bool FOUR>
+template <int FORM, int NT, int P, int S, bool FOUR, int WH>
 __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
-  using K = SCfg<FORM, NT, P, S>;
+  using K = SCfg<FORM, NT, P, S, WH>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* xring = smem;
@@ -261,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
       if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
       uint8_t* ys = yring + (size_t)s * K::kStageY;
-      for (int z = lane; z < P * kYBytes / 16; z += 32)
+      for (int z = lane; z < P * K::kYB / 16; z += 32)
         reinterpret_cast<float4*>(ys)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
       __syncwarp();
       const int32_t e0 = off[0], e1 = off[nb];
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
         for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
         const uint32_t pos = __ldg(p.tile + e);
         const float v = p.vals ? __ldg(p.vals + e) : 1.0f;
-        if (pos >= kWinH * kBlkW) {
+        if (pos >= WH * kBlkW) {
           atomicOr(p.err, kErrBadIndex);
           continue;
         }
@@ -280,11 +284,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
         const __nv_bfloat16 hi = __float2bfloat16_rn(v);
         const uint16_t hb = __bfloat16_as_ushort(hi);
         const uint16_t lb = bf16_bits(v - __bfloat162float(hi));
-        uint8_t* yb = ys + pb * kYBytes;
+        uint8_t* yb = ys + pb * K::kYB;
         *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, sl)) = hb;
         *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, 8 + sl)) = hb;
-        *reinterpret_cast<uint16_t*>(yb + ysplit_offset(16 + r, sl)) = lb;
-        if (FOUR) *reinterpret_cast<uint16_t*>(yb + ysplit_offset(16 + r, 8 + sl)) = lb;
+        *reinterpret_cast<uint16_t*>(yb + ysplit_offset(WH + r, sl)) = lb;
+        if (FOUR) *reinterpret_cast<uint16_t*>(yb + ysplit_offset(WH + r, 8 + sl)) = lb;
       }
       fence_proxy_async_smem();
       __syncwarp();
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const int m = warp - kMmaWarp;
       int32_t ws, we;
       cta_windows(p, c, b0, b1, ws, we);
-      constexpr uint32_t idesc = umma_idesc(1, 128, 32, 1, 0);
+      constexpr uint32_t idesc = umma_idesc(1, 128, 2 * WH, 1, 0);
       const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 2048, 2);
       const uint64_t bdesc0 = umma_desc(smem_u32(yring), 128, 256, 0);
       uint32_t q = 0;
@@ -433,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
         const int a = (int)(q % K::kNacc);
         if (!mbar_wait(&acc_empty[a], ((q / K::kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t dtm = tmem_base + (uint32_t)((m * K::kNacc + a) * NT * 32);
+        const uint32_t dtm = tmem_base + (uint32_t)((m * K::kNacc + a) * K::kAccCols);
         uint32_t acc = 0;
         int64_t st = (s0 - b0) / P;
         st += (m - (int)(st % kMmaWarps) + kMmaWarps) % kMmaWarps;
@@ -448,16 +452,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
             fence_proxy_async_smem();
             tc_fence_after();
           }
-          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * kYBytes) >> 4);
+          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * K::kYB) >> 4);
           uint64_t adesc =
               adesc0 + (uint64_t)((s * K::kStageX + (int)(lo - sb) * NT * kTileBytes) >> 4);
           for (int64_t b = lo; b < hi; ++b) {
 #pragma unroll
             for (int t = 0; t < NT; ++t)
-              mma_f16(dtm + t * 32, adesc + (uint64_t)(t * (kTileBytes >> 4)), bdesc, idesc, acc);
+              mma_f16(dtm + t * 2 * WH, adesc + (uint64_t)(t * (kTileBytes >> 4)), bdesc, idesc,
+                      acc);
             acc = 1;
             adesc += (uint64_t)((NT * kTileBytes) >> 4);
-            bdesc += (uint64_t)(kYBytes >> 4);
+            bdesc += (uint64_t)(K::kYB >> 4);
           }
           if (hi == sb + P || hi == b1) tc_commit(&empty[s]);
         }
@@ -480,10 +485,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const int64_t r0 = rn0, r1 = rn1;
       rn0 = rn1;
       rn1 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;
-      const int64_t row0 = (int64_t)w * kWinH;
+      const int64_t row0 = (int64_t)w * WH;
       if (r0 == r1) {
         for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
-          for (int r = 0; r < kWinH && row0 + r < p.M; ++r)
+          for (int r = 0; r < WH && row0 + r < p.M; ++r)
             p.C[(row0 + r) * p.N + f] = epilogue(p, 0.0f, f);
         continue;
       }
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       bool guard_rows = true;
       if (p.mode == 1 && (r0 < b0 || r1 > b1)) {
         const int slot = (r0 < b0) ? 2 * c : 2 * c + 1;
-        out = p.part + (size_t)slot * kWinH * p.N;
+        out = p.part + (size_t)slot * WH * p.N;
         guard_rows = false;
       } else {
         out = p.C + row0 * p.N;
@@ -508,32 +513,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const uint32_t lane_addr = tmem_base + ((uint32_t)(ew * 32) << 16);
 #pragma unroll 1
       for (int t = 0; t < NT; ++t) {
-        float x[16];
-#pragma unroll
-        for (int r = 0; r < kWinH; ++r) x[r] = 0.0f;
-        // fixed order: issuer 0's partial, then issuer 1's
-#pragma unroll 1
-        for (int mi = 0; mi < kMmaWarps; ++mi) {
-          if (!both && mi != m0) continue;
-          uint32_t v[16], u[16];
-          const uint32_t col = (uint32_t)(((mi * K::kNacc + a) * NT + t) * 32);
-          tmem_ld16(lane_addr + col, v);
-          tmem_ld16(lane_addr + col + 16, u);
-          tmem_ld_wait();
-#pragma unroll
-          for (int r = 0; r < kWinH; ++r) x[r] += __uint_as_float(v[r]) + __uint_as_float(u[r]);
-        }
         const int f = col0 + t * 128 + ew * 32 + lane;
-        if (t == NT - 1) {
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[a]);
-        }
-        if (f < p.N) {
+#pragma unroll 1
+        for (int h = 0; h < WH / 16; ++h) {  // 16 window rows at a time
+          float x[16];
 #pragma unroll
-          for (int r = 0; r < kWinH; ++r)
-            if (!guard_rows) out[r * p.N + f] = x[r];  // partial tile: raw sum
-            else if (row0 + r < p.M) out[r * p.N + f] = epilogue(p, x[r], f);
+          for (int r = 0; r < 16; ++r) x[r] = 0.0f;
+          // fixed order: issuer 0's partial, then issuer 1's
+#pragma unroll 1
+          for (int mi = 0; mi < kMmaWarps; ++mi) {
+            if (!both && mi != m0) continue;
+            uint32_t v[16], u[16];
+            const uint32_t col = (uint32_t)((mi * K::kNacc + a) * K::kAccCols + t * 2 * WH);
+            tmem_ld16(lane_addr + col + h * 16, v);       // A_hi columns
+            tmem_ld16(lane_addr + col + WH + h * 16, u);  // A_lo columns
+            tmem_ld_wait();
+#pragma unroll
+            for (int r = 0; r < 16; ++r) x[r] += __uint_as_float(v[r]) + __uint_as_float(u[r]);
+          }
+          if (t == NT - 1 && h == WH / 16 - 1) {
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[a]);
+          }
+          if (f < p.N) {
+            float* o = out + (size_t)h * 16 * p.N;
+            const int64_t rb = row0 + h * 16;
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+              if (!guard_rows) o[r * p.N + f] = x[r];  // partial tile: raw sum
+              else if (rb + r < p.M) o[r * p.N + f] = epilogue(p, x[r], f);
+          }
         }
       }
       ++q;
@@ -548,20 +558,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
   }
 }
 
-template <int FORM, int NT, int P, int S, bool FOUR>
+template <int FORM, int NT, int P, int S, bool FOUR, int WH>
 dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
-  constexpr int smem = SCfg<FORM, NT, P, S>::kSmem;
+  constexpr int smem = SCfg<FORM, NT, P, S, WH>::kSmem;
   static_assert(smem <= 227 * 1024, "shared memory budget");
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    DTC_CUDA(cudaFuncSetAttribute(k_spmm_split<FORM, NT, P, S, FOUR>,
+    DTC_CUDA(cudaFuncSetAttribute(k_spmm_split<FORM, NT, P, S, FOUR, WH>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set[dev & 63] = true;
   }
   dim3 grid((unsigned)p.G, (unsigned)slices);
-  k_spmm_split<FORM, NT, P, S, FOUR><<<grid, kThreads, smem, st>>>(p);
+  k_spmm_split<FORM, NT, P, S, FOUR, WH><<<grid, kThreads, smem, st>>>(p);
   DTC_CUDA(cudaGetLastError());
   if (p.mode == 1 && p.G > 1) {
     k_reduce_partials<<<p.G - 1, 256, 0, st>>>(p);
@@ -570,13 +580,19 @@ dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
   return DTC_OK;
 }
 
+// N-tiles per CTA: all of N up to 4 (window height 16) or 2 (height 32, whose
+// accumulators are twice as wide) unless capped by `ntile`.
 template <int FORM, bool FOUR>
 dtc_status dispatch_n(const Params& p, cudaStream_t st, int ntile) {
   int nt = p.N <= 128 ? 1 : p.N <= 256 ? 2 : 4;
   if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
-  if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR>(p, (p.N + 127) / 128, st);
-  if (nt == 2) return launch_split<FORM, 2, 2, 8, FOUR>(p, (p.N + 255) / 256, st);
-  return launch_split<FORM, 4, 1, 8, FOUR>(p, (p.N + 511) / 512, st);
+  if (p.H == 32) {
+    if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
+    return launch_split<FORM, 2, 2, 8, FOUR, 32>(p, (p.N + 255) / 256, st);
+  }
+  if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 16>(p, (p.N + 127) / 128, st);
+  if (nt == 2) return launch_split<FORM, 2, 2, 8, FOUR, 16>(p, (p.N + 255) / 256, st);
+  return launch_split<FORM, 4, 1, 8, FOUR, 16>(p, (p.N + 511) / 512, st);
 }
 
 }  // namespace
@@ -585,7 +601,7 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile, Epilogue epi) {
+                           cudaStream_t st, int ntile, Epilogue epi, int H) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8,
               "split kernels take SPLIT24, BF16 or FP8 B");
@@ -594,7 +610,8 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   DTC_REQUIRE(N % 16 == 0, "split forms need N % 16 == 0 (16-byte row segments of every plane)");
   DTC_REQUIRE(bformat == DTC_B_BF16 || p1 != nullptr, "second B plane missing");
   DTC_REQUIRE(((uintptr_t)p0 & 15) == 0 && ((uintptr_t)p1 & 15) == 0, "planes must be 16-byte aligned");
-  DTC_REQUIRE(nwin == (M + kWinH - 1) / kWinH, "num_windows must be ceil(num_nodes/16)");
+  DTC_REQUIRE(H == 16 || H == 32, "window height must be 16 or 32");
+  DTC_REQUIRE(nwin == (M + H - 1) / H, "num_windows must be ceil(num_nodes / window height)");
   DTC_REQUIRE(mode == 0 || part != nullptr, "balance mode needs the partials workspace");
   if (!is_sm100()) {
     set_error("tcgen05 kernels need an sm_100 device");
@@ -610,18 +627,21 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   p.B = reinterpret_cast<const float*>(p0); p.B1 = p1; p.bformat = bformat;
   p.C = C; p.part = part; p.err = device_error_word();
   p.bias = epi.bias; p.relu = epi.relu;
-  p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
+  p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode; p.H = H;
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
   const bool four = precision == DTC_PREC_SPLIT4;
   switch (bformat) {
     case DTC_B_SPLIT24:
-      return four ? dispatch_n<kFormSplit24, true>(p, st, ntile) : dispatch_n<kFormSplit24, false>(p, st, ntile);
+      return four ? dispatch_n<kFormSplit24, true>(p, st, ntile)
+                  : dispatch_n<kFormSplit24, false>(p, st, ntile);
     case DTC_B_BF16:
-      return four ? dispatch_n<kFormBF16, true>(p, st, ntile) : dispatch_n<kFormBF16, false>(p, st, ntile);
+      return four ? dispatch_n<kFormBF16, true>(p, st, ntile)
+                  : dispatch_n<kFormBF16, false>(p, st, ntile);
     default:
-      return four ? dispatch_n<kFormFP8, true>(p, st, ntile) : dispatch_n<kFormFP8, false>(p, st, ntile);
+      return four ? dispatch_n<kFormFP8, true>(p, st, ntile)
+                  : dispatch_n<kFormFP8, false>(p, st, ntile);
   }
 }
 

@@ -51,9 +51,7 @@ constexpr int kLoadWarps = 4;
 constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;
 constexpr int kTileWarps = 4;
 constexpr int kThreads = 32 * (kTileWarp0 + kTileWarps);  // 448
-constexpr int kNacc = 4;        // TMEM accumulator buffers in flight
 constexpr int kXTileBytes = 4096;   // 8 rows x 128 fp32 features
-constexpr int kYBytes = 512;        // 16 x 8 fp32, K-major core matrices
 
 // Byte offset, inside one 8-row x 128-feature fp32 tile, of 16-byte chunk
 // `cc` (features 4cc..4cc+3) of row k, in the UMMA layout-type-1 atom order:
@@ -64,26 +62,30 @@ __device__ __forceinline__ uint32_t x_offset_tf32(uint32_t k, uint32_t cc) {
   return a * 1024 + (k >> 2) * 512 + (k & 3) * 128 + ((g << 1) | (j & 1)) * 16;
 }
 
-template <int NT, int P, int S>
+// WH = row-window height (the UMMA N dimension): 16 or 32.
+template <int NT, int P, int S, int WH>
 struct Cfg {
   static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kMmaWarps == 0,
                 "stage ownership");
   static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
+  static_assert(WH == 16 || WH == 32, "window height");
+  static constexpr int kNacc = (NT * WH > 64) ? 2 : 4;  // TMEM accumulator buffers in flight
+  static constexpr int kYB = WH * kBlkW * 4;            // WH x 8 fp32, K-major core matrices
   static constexpr int kStageX = P * NT * kXTileBytes;
-  static constexpr int kStageY = P * kYBytes;
+  static constexpr int kStageY = P * kYB;
   static constexpr int kX = S * kStageX;
   static constexpr int kY = S * kStageY;
   static constexpr int kBars = (2 * S + 2 * kNacc) * 8;
   static constexpr int kSmem = kX + kY + kBars + 16 + 1024;  // + alignment slack
-  static constexpr int kCols = kMmaWarps * kNacc * NT * 16;  // TMEM columns used
+  static constexpr int kCols = kMmaWarps * kNacc * NT * WH;  // TMEM columns used
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
                                         : kCols <= 256 ? 256 : 512;
 };
 
-template <int NT, int P, int S>
+template <int NT, int P, int S, int WH>
 __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
-  using K = Cfg<NT, P, S>;
+  using K = Cfg<NT, P, S, WH>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* xring = smem;
@@ -92,8 +94,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
   uint64_t* full = bars;                 // [S] 32 cp.async arrivals + 1 tile arrival
   uint64_t* empty = bars + S;            // [S] UMMA commit
   uint64_t* acc_full = bars + 2 * S;     // [kNacc] UMMA commit
-  uint64_t* acc_empty = acc_full + kNacc;  // [kNacc] 4 epilogue warps
-  uint32_t* tmem_slot = (uint32_t*)(acc_empty + kNacc);
+  uint64_t* acc_empty = acc_full + K::kNacc;  // [kNacc] 4 epilogue warps
+  uint32_t* tmem_slot = (uint32_t*)(acc_empty + K::kNacc);
   volatile uint32_t* abort_flag = tmem_slot + 1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -107,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       mbar_init(&full[i], 32 + 1);
       mbar_init(&empty[i], 1);
     }
-    for (int i = 0; i < kNacc; ++i) {
+    for (int i = 0; i < K::kNacc; ++i) {
       mbar_init(&acc_full[i], kMmaWarps);
       mbar_init(&acc_empty[i], kEpiWarps);
     }
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
       uint8_t* ys = yring + (size_t)s * K::kStageY;
 #pragma unroll
-      for (int z = lane; z < P * kYBytes / 16; z += 32)
+      for (int z = lane; z < P * K::kYB / 16; z += 32)
         reinterpret_cast<float4*>(ys)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
       __syncwarp();
       const int32_t e0 = off[0], e1 = off[nb];
@@ -210,11 +212,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
         for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
         const uint32_t pos = __ldg(p.tile + e);
         const float v = p.vals ? __ldg(p.vals + e) : 1.0f;
-        if (pos < kWinH * kBlkW) {
+        if (pos < WH * kBlkW) {
           if (v != 0.0f) {
             uint32_t t32;
             asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(t32) : "f"(v));
-            *reinterpret_cast<uint32_t*>(ys + pb * kYBytes + y_offset(pos)) = t32;
+            *reinterpret_cast<uint32_t*>(ys + pb * K::kYB + y_offset(pos)) = t32;
           }
         } else {
           atomicOr(p.err, kErrBadIndex);
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       const int m = warp - kMmaWarp;  // this issuer's stages: st % kMmaWarps == m
       int32_t ws, we;
       cta_windows(p, c, b0, b1, ws, we);
-      constexpr uint32_t idesc = umma_idesc(2, 128, 16, 1, 0);
+      constexpr uint32_t idesc = umma_idesc(2, 128, WH, 1, 0);
       // Descriptors advance by adding (byte offset >> 4) to the start-address
       // field (shared addresses < 256 KB fit its 14 bits, no carry out).
       const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 512, 1);
@@ -246,10 +248,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
         r0 = r1;
         r1 = r2;
         if (s0 >= s1) continue;  // empty window, or no blocks of it in this range
-        const int a = (int)(q % kNacc);
-        if (!mbar_wait(&acc_empty[a], ((q / kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
+        const int a = (int)(q % K::kNacc);
+        if (!mbar_wait(&acc_empty[a], ((q / K::kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t dtm = tmem_base + (uint32_t)((m * kNacc + a) * NT * 16);
+        const uint32_t dtm = tmem_base + (uint32_t)((m * K::kNacc + a) * NT * WH);
         uint32_t acc = 0;
         // this issuer's stages that intersect [s0, s1)
         int64_t st = (s0 - b0) / P;
@@ -265,16 +267,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
             fence_proxy_async_smem();  // cp.async (generic proxy) data -> UMMA reads
             tc_fence_after();
           }
-          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * kYBytes) >> 4);
+          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * K::kYB) >> 4);
           uint64_t adesc =
               adesc0 + (uint64_t)((s * K::kStageX + (int)(lo - sb) * NT * kXTileBytes) >> 4);
           for (int64_t b = lo; b < hi; ++b) {
 #pragma unroll
             for (int t = 0; t < NT; ++t)
-              mma_tf32(dtm + t * 16, adesc + (uint64_t)(t * (kXTileBytes >> 4)), bdesc, idesc, acc);
+              mma_tf32(dtm + t * WH, adesc + (uint64_t)(t * (kXTileBytes >> 4)), bdesc, idesc, acc);
             acc = 1;
             adesc += (uint64_t)((NT * kXTileBytes) >> 4);
-            bdesc += (uint64_t)(kYBytes >> 4);
+            bdesc += (uint64_t)(K::kYB >> 4);
           }
           if (hi == sb + P || hi == b1) tc_commit(&empty[s]);  // stage fully consumed
         }
@@ -297,23 +299,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       const int64_t r0 = rn0, r1 = rn1;
       rn0 = rn1;
       rn1 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;  // prefetch the next window's end
-      const int64_t row0 = (int64_t)w * kWinH;
+      const int64_t row0 = (int64_t)w * WH;
       if (r0 == r1) {  // empty window: C rows are zero
         for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
-          for (int r = 0; r < kWinH && row0 + r < p.M; ++r)
+          for (int r = 0; r < WH && row0 + r < p.M; ++r)
             p.C[(row0 + r) * p.N + f] = epilogue(p, 0.0f, f);
         continue;
       }
       if ((r0 > b0 ? r0 : b0) >= (r1 < b1 ? r1 : b1)) continue;
-      const int a = (int)(q % kNacc);
-      const bool got = mbar_wait(&acc_full[a], (q / kNacc) & 1, p.err);
+      const int a = (int)(q % K::kNacc);
+      const bool got = mbar_wait(&acc_full[a], (q / K::kNacc) & 1, p.err);
       if (!__all_sync(0xffffffffu, got)) { *abort_flag = 1; break; }
       tc_fence_after();
       float* out;
       bool guard_rows = true;
       if (p.mode == 1 && (r0 < b0 || r1 > b1)) {  // window cut by a CTA boundary
         const int slot = (r0 < b0) ? 2 * c : 2 * c + 1;
-        out = p.part + (size_t)slot * kWinH * p.N;
+        out = p.part + (size_t)slot * WH * p.N;
         guard_rows = false;
       } else {
         out = p.C + row0 * p.N;
@@ -325,20 +327,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
       const int m0 = (int)(st0 % kMmaWarps);
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        uint32_t v[16], u[16];
+        uint32_t v[WH / 16][16], u[WH / 16][16];
         const uint32_t lane_addr = tmem_base + ((uint32_t)(ew * 32) << 16);
-        tmem_ld16(lane_addr + (uint32_t)(((m0 * kNacc + a) * NT + t) * 16), v);
-        if (both) tmem_ld16(lane_addr + (uint32_t)((((1 - m0) * kNacc + a) * NT + t) * 16), u);
+        const uint32_t c0 = (uint32_t)(((m0 * K::kNacc + a) * NT + t) * WH);
+        const uint32_t c1 = (uint32_t)((((1 - m0) * K::kNacc + a) * NT + t) * WH);
+#pragma unroll
+        for (int h = 0; h < WH / 16; ++h) {
+          tmem_ld16(lane_addr + c0 + h * 16, v[h]);
+          if (both) tmem_ld16(lane_addr + c1 + h * 16, u[h]);
+        }
         tmem_ld_wait();
-        float x[16];
+        float x[WH];
         if (both) {  // fixed order: issuer 0's partial + issuer 1's partial
 #pragma unroll
-          for (int r = 0; r < kWinH; ++r)
-            x[r] = m0 == 0 ? __uint_as_float(v[r]) + __uint_as_float(u[r])
-                           : __uint_as_float(u[r]) + __uint_as_float(v[r]);
+          for (int r = 0; r < WH; ++r) {
+            const float pv = __uint_as_float(v[r >> 4][r & 15]);
+            const float pu = __uint_as_float(u[r >> 4][r & 15]);
+            x[r] = m0 == 0 ? pv + pu : pu + pv;
+          }
         } else {
 #pragma unroll
-          for (int r = 0; r < kWinH; ++r) x[r] = __uint_as_float(v[r]);
+          for (int r = 0; r < WH; ++r) x[r] = __uint_as_float(v[r >> 4][r & 15]);
         }
         const int f = col0 + t * 128 + ew * 32 + lane;
         if (t == NT - 1) {
@@ -348,7 +357,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const Params p) {
         }
         if (f < p.N) {
 #pragma unroll
-          for (int r = 0; r < kWinH; ++r)
+          for (int r = 0; r < WH; ++r)
             if (!guard_rows) out[r * p.N + f] = x[r];  // partial tile: raw sum
             else if (row0 + r < p.M) out[r * p.N + f] = epilogue(p, x[r], f);
         }
@@ -375,20 +384,20 @@ __global__ void k_rowid_to_rwo(const int32_t* __restrict__ rowid, int64_t T, int
   }
 }
 
-template <int NT, int P, int S>
+template <int NT, int P, int S, int WH>
 dtc_status launch_tf32(const Params& p, int slices, cudaStream_t st) {
-  constexpr int smem = Cfg<NT, P, S>::kSmem;
+  constexpr int smem = Cfg<NT, P, S, WH>::kSmem;
   static_assert(smem <= 227 * 1024, "shared memory budget");
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    DTC_CUDA(cudaFuncSetAttribute(k_spmm_tf32<NT, P, S>,
+    DTC_CUDA(cudaFuncSetAttribute(k_spmm_tf32<NT, P, S, WH>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set[dev & 63] = true;
   }
   dim3 grid((unsigned)p.G, (unsigned)slices);
-  k_spmm_tf32<NT, P, S><<<grid, kThreads, smem, st>>>(p);
+  k_spmm_tf32<NT, P, S, WH><<<grid, kThreads, smem, st>>>(p);
   DTC_CUDA(cudaGetLastError());
   if (p.mode == 1 && p.G > 1) {
     k_reduce_partials<<<p.G - 1, 256, 0, st>>>(p);
@@ -403,11 +412,12 @@ dtc_status launch_tf32(const Params& p, int slices, cudaStream_t st) {
 dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                           const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                           int64_t T, const float* B, int32_t N, float* C, int mode, int grid,
-                          float* part, cudaStream_t st, int ntile, Epilogue epi) {
+                          float* part, cudaStream_t st, int ntile, Epilogue epi, int H) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(N % 4 == 0, "tcgen05 path needs N % 4 == 0 (16-byte row segments)");
   DTC_REQUIRE(((uintptr_t)B & 15) == 0, "B must be 16-byte aligned");
-  DTC_REQUIRE(nwin == (M + kWinH - 1) / kWinH, "num_windows must be ceil(num_nodes/16)");
+  DTC_REQUIRE(H == 16 || H == 32, "window height must be 16 or 32");
+  DTC_REQUIRE(nwin == (M + H - 1) / H, "num_windows must be ceil(num_nodes / window height)");
   if (!is_sm100()) {
     set_error("tcgen05 kernels need an sm_100 device");
     return DTC_ERR_UNSUPPORTED;
@@ -421,7 +431,7 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
   p.rwo = rwo; p.tile = tile; p.toff = toff; p.s2x = s2x; p.vals = vals; p.B = B;
   p.C = C; p.part = part; p.err = device_error_word();
   p.bias = epi.bias; p.relu = epi.relu;
-  p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode;
+  p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode; p.H = H;
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
@@ -429,15 +439,20 @@ dtc_status spmm_tf32_impl(const int32_t* rwo, const uint8_t* tile, const int32_t
   // by `ntile`; wider slices of N go to more CTAs (grid.y).
   int nt = N <= 128 ? 1 : N <= 256 ? 2 : 4;
   if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
-  if (nt == 1) return launch_tf32<1, 4, 8>(p, (N + 127) / 128, st);
-  if (nt == 2) return launch_tf32<2, 2, 8>(p, (N + 255) / 256, st);
-  return launch_tf32<4, 1, 8>(p, (N + 511) / 512, st);
+  if (H == 32) {
+    if (nt == 1) return launch_tf32<1, 4, 8, 32>(p, (N + 127) / 128, st);
+    if (nt == 2) return launch_tf32<2, 2, 8, 32>(p, (N + 255) / 256, st);
+    return launch_tf32<4, 1, 8, 32>(p, (N + 511) / 512, st);
+  }
+  if (nt == 1) return launch_tf32<1, 4, 8, 16>(p, (N + 127) / 128, st);
+  if (nt == 2) return launch_tf32<2, 2, 8, 16>(p, (N + 255) / 256, st);
+  return launch_tf32<4, 1, 8, 16>(p, (N + 511) / 512, st);
 }
 
-size_t spmm_partials_bytes(int64_t T, int32_t N, int grid) {
+size_t spmm_partials_bytes(int64_t T, int32_t N, int grid, int H) {
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)(T > 0 ? T : 1);
-  return (size_t)2 * G * kWinH * (size_t)N * sizeof(float);
+  return (size_t)2 * G * H * (size_t)N * sizeof(float);
 }
 
 dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,

@@ -26,12 +26,16 @@ namespace {
 constexpr int kWaveChoices[] = {1, 2, 4, 8, 16};
 constexpr int kMaxWaves = 16;
 
-int auto_ntile(int32_t N) { return N <= 128 ? 1 : N <= 256 ? 2 : 4; }
+// N-tiles per CTA when the caller does not cap them (see the kernels' dispatch).
+int auto_ntile(int32_t N, int H, bool split) {
+  const int nt = N <= 128 ? 1 : N <= 256 ? 2 : 4;
+  return (split && H == 32 && nt > 2) ? 2 : nt;
+}
 
 // Every distinct (mode, waves, ntile) the kernels support for this N.
-int candidates(int32_t N, dtc_schedule* out, int max) {
+int candidates(int32_t N, int H, bool split, dtc_schedule* out, int max) {
   int n = 0;
-  const int nt_auto = auto_ntile(N);
+  const int nt_auto = auto_ntile(N, H, split);
   for (int mode = 0; mode <= 1; ++mode)
     for (int w : kWaveChoices)
       for (int nt = 1; nt <= 4; nt *= 2) {
@@ -63,21 +67,28 @@ extern "C" {
 
 int dtc_schedule_candidates(int32_t N, dtc_schedule* out, int max_out) {
   if (N < 1) return 0;
-  return candidates(N, out, max_out);
+  return candidates(N, 16, false, out, max_out);
+}
+
+int dtc_schedule_candidates_ex(int32_t N, int32_t block_h, int split, dtc_schedule* out,
+                               int max_out) {
+  if (N < 1 || (block_h != 16 && block_h != 32)) return 0;
+  return candidates(N, block_h, split != 0, out, max_out);
 }
 
 dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
-                                        size_t* bytes) {
+                                        int32_t block_h, size_t* bytes) {
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
-  *bytes = spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms());
+  DTC_REQUIRE(block_h == 16 || block_h == 32, "block_h must be 16 or 32");
+  *bytes = spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms(), block_h);
   return DTC_OK;
 }
 
 dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                         const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                         const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                        int64_t num_blocks, int bformat, const void* d_Bplane0,
+                        int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                         const void* d_Bplane1, int32_t N, int precision, float* d_C,
                         void* d_workspace, size_t workspace_bytes, int reps,
                         dtc_schedule* results, int max_results, int* num_results, int* best,
@@ -87,7 +98,7 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
   DTC_REQUIRE(reps >= 1 && reps <= 1000, "reps must be in [1, 1000]");
   DTC_REQUIRE(best != nullptr, "best is null");
   size_t need = 0;
-  dtc_status s = dtc_autotune_workspace_bytes(num_nodes, num_blocks, N, &need);
+  dtc_status s = dtc_autotune_workspace_bytes(num_nodes, num_blocks, N, block_h, &need);
   if (s != DTC_OK) return s;
   if (!d_workspace || workspace_bytes < need) {
     set_error("autotune workspace too small (dtc_autotune_workspace_bytes)");
@@ -99,9 +110,9 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
   } else {
     DTC_REQUIRE(N % 16 == 0, "split-precision path needs N % 16 == 0");
   }
-  const int ncand = candidates(N, nullptr, 0);
+  const int ncand = candidates(N, block_h, !tf32, nullptr, 0);
   std::vector<dtc_schedule> cand(ncand);
-  candidates(N, cand.data(), ncand);
+  candidates(N, block_h, !tf32, cand.data(), ncand);
   cudaStream_t st = (cudaStream_t)stream;
   Events ev;
   DTC_CUDA(cudaEventCreate(&ev.a));
@@ -117,11 +128,11 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
       return tf32 ? spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
                                    d_tcValues, num_nodes, num_windows, num_blocks,
                                    (const float*)d_Bplane0, N, d_C, c.mode, c.grid,
-                                   (float*)d_workspace, st, c.ntile)
+                                   (float*)d_workspace, st, c.ntile, Epilogue{}, block_h)
                   : spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
                                     d_tcValues, num_nodes, num_windows, num_blocks, bformat,
                                     d_Bplane0, d_Bplane1, N, precision, d_C, c.mode, c.grid,
-                                    (float*)d_workspace, st, c.ntile);
+                                    (float*)d_workspace, st, c.ntile, Epilogue{}, block_h);
     };
     s = run();  // warm-up
     if (s != DTC_OK) return s;

@@ -33,16 +33,17 @@ SIGNATURES = {
     "dtc_spmm": [vp, vp, vp, vp, vp, i32, i32, i64, vp, i32, vp, vp],
     "dtc_spmm_balance_workspace_bytes": [i32, i64, i32, szp],
     "dtc_spmm_balance": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp, sz, vp],
-    "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
+    "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp,
                     C.c_int, C.c_int, C.c_int, vp, sz, vp],
-    "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, C.c_int, C.c_int, szp],
-    "dtc_spmm_fused": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp,
+    "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, i32, C.c_int, C.c_int, szp],
+    "dtc_spmm_fused": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp,
                        C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
     "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
     "dtc_spmm_balance_noalloc": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp],
     "dtc_noalloc_scratch_capacity": [],
     "dtc_schedule_candidates": [i32, vp, C.c_int],
+    "dtc_schedule_candidates_ex": [i32, i32, C.c_int, vp, C.c_int],
     "dtc_relabel_workspace_bytes": [i32, i32, i64, szp],
     "dtc_tca_default_params": [vp],
     "dtc_features_workspace_bytes": [],
@@ -58,12 +59,13 @@ SIGNATURES = {
     "dtc_permute_csr": [vp, vp, vp, i32, i64, vp, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_transpose_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_coo_to_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
-    "dtc_autotune_workspace_bytes": [i32, i64, i32, szp],
-    "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, C.c_int, vp, vp, i32, C.c_int, vp, vp, sz,
+    "dtc_autotune_workspace_bytes": [i32, i64, i32, i32, szp],
+    "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp, vp, sz,
                      C.c_int, vp, C.c_int, vp, vp, vp],
 }
 _RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int,
              "dtc_noalloc_scratch_capacity": C.c_size_t, "dtc_schedule_candidates": C.c_int,
+             "dtc_schedule_candidates_ex": C.c_int,
              "dtc_tca_default_params": None, "dtc_features_workspace_bytes": C.c_size_t,
              "dtc_mlp_num_params": C.c_int64, "dtc_mlp_backward_workspace_bytes": C.c_size_t}
 

@@ -150,16 +150,18 @@ def pack_b_into(B: torch.Tensor, fmt: int, planes):
 
 def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True, out=None,
             workspace=None, ntile=0):
+    if m.W != 8:
+        raise ValueError("the SpMM kernels take TC blocks of width 8")
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     wsb = C.c_size_t()
-    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, mode, grid, C.byref(wsb))
+    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, m.H, mode, grid, C.byref(wsb))
     ws = workspace
     if ws is None and wsb.value:
         ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
     vals = m.TCvalues if use_values else None
     call("dtc_spmm_ex", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId), _ptr(m.TCblockoffset),
-         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, fmt, _ptr(planes[0]),
+         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt, _ptr(planes[0]),
          _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(C_), mode, grid,
          ntile, _ptr(ws), 0 if ws is None else ws.numel(), _stream())
     return C_
@@ -168,17 +170,19 @@ def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True
 def spmm_fused(m: METCF, planes, fmt, N, precision, bias=None, relu=False, mode=0, grid=0,
                ntile=0, use_values=True, out=None, workspace=None):
     """spmm_ex with C = act(A*B + bias) fused into the store of C (GCN epilogue)."""
+    if m.W != 8:
+        raise ValueError("the SpMM kernels take TC blocks of width 8")
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     wsb = C.c_size_t()
-    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, mode, grid, C.byref(wsb))
+    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, m.H, mode, grid, C.byref(wsb))
     ws = workspace
     if ws is None and wsb.value:
         ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
     vals = m.TCvalues if use_values else None
     bias = None if bias is None else bias.to(torch.float32).contiguous()
     call("dtc_spmm_fused", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId),
-         _ptr(m.TCblockoffset), _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, fmt,
+         _ptr(m.TCblockoffset), _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt,
          _ptr(planes[0]), _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(bias),
          1 if relu else 0, _ptr(C_), mode, grid, ntile, _ptr(ws), 0 if ws is None else ws.numel(),
          _stream())

@@ -31,18 +31,19 @@ FORMS = {
 }
 
 
-def candidates(N):
-    """Every (mode, waves, ntile) schedule the kernels support for width N."""
+def candidates(N, H=16, split=False):
+    """Every (mode, waves, ntile) schedule the kernels support for width N at
+    window height H (split: the split-precision kernels)."""
     L = _lib.lib()
-    n = L.dtc_schedule_candidates(N, None, 0)
+    n = L.dtc_schedule_candidates_ex(N, H, 1 if split else 0, None, 0)
     arr = (Schedule * n)()
-    L.dtc_schedule_candidates(N, arr, n)
+    L.dtc_schedule_candidates_ex(N, H, 1 if split else 0, arr, n)
     return list(arr)
 
 
 def workspace_for(m: METCF, N, device):
     b = C.c_size_t()
-    call("dtc_autotune_workspace_bytes", m.M, m.T, N, C.byref(b))
+    call("dtc_autotune_workspace_bytes", m.M, m.T, N, m.H, C.byref(b))
     return torch.empty(max(b.value, 1), dtype=torch.uint8, device=device)
 
 
@@ -52,12 +53,12 @@ def autotune(m: METCF, planes, fmt, N, precision, reps=3, use_values=True, out=N
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     ws = workspace if workspace is not None else workspace_for(m, N, dev)
-    ncand = len(candidates(N))
+    ncand = len(candidates(N, m.H, not (fmt == B_F32 and precision == PREC_TF32)))
     res = (Schedule * ncand)()
     nres, best = C.c_int(), C.c_int()
     vals = m.TCvalues if use_values else None
     call("dtc_autotune", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId), _ptr(m.TCblockoffset),
-         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, fmt, _ptr(planes[0]),
+         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt, _ptr(planes[0]),
          _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(C_), _ptr(ws),
          ws.numel(), reps, res, ncand, C.byref(nres), C.byref(best), _stream())
     out_list = list(res)[: nres.value]

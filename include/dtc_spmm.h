@@ -220,20 +220,22 @@ dtc_status dtc_spmm_balance_noalloc(const int32_t* d_tcblockRowid, const uint8_t
 size_t dtc_noalloc_scratch_capacity(void);
 
 /* General form used by the tuned paths: any B format / precision, explicit
- * schedule. mode 0 = window-scheduled, 1 = strict balance. grid = CTAs (0 =
- * 16 per SM, run as waves). ntile = 128-feature tiles per CTA (0 = all of N
- * up to 4; 1 or 2 split wider N across more CTAs). d_rowWindowOffset is
- * required (build it from TCblockRowid with dtc_rowid_to_window_offset).
- * Workspace needed only for mode 1. */
+ * schedule. block_h = row-window height of the ME-TCF arrays (16 or 32; the
+ * conversion's blockSize_h, with blockSize_w = 8). mode 0 = window-scheduled,
+ * 1 = strict balance. grid = CTAs (0 = 16 per SM, run as waves). ntile =
+ * 128-feature tiles per CTA (0 = all of N up to 4, or up to 2 for the split
+ * forms at block_h 32; 1 or 2 split wider N across more CTAs).
+ * d_rowWindowOffset is required (build it from TCblockRowid with
+ * dtc_rowid_to_window_offset). Workspace needed only for mode 1. */
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                       int64_t num_blocks, int bformat, const void* d_Bplane0,
+                       int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                        const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
                        int grid, int ntile, void* d_workspace, size_t workspace_bytes,
                        dtc_stream_t stream);
-dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N, int mode,
-                                       int grid, size_t* bytes);
+dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
+                                       int32_t block_h, int mode, int grid, size_t* bytes);
 
 /* dtc_spmm_ex with the GCN layer's epilogue fused into the store of C:
  * C = act(A*B + bias), bias[N] per column (NULL = none), act = ReLU when
@@ -242,7 +244,7 @@ dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, in
 dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                           const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                           const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                          int64_t num_blocks, int bformat, const void* d_Bplane0,
+                          int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                           const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
                           int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
                           size_t workspace_bytes, dtc_stream_t stream);
@@ -264,10 +266,14 @@ typedef struct {
 /* Fills out[0..min(count, max_out)) with every schedule the kernels support for
  * N and returns the count (out may be NULL to query it). */
 int dtc_schedule_candidates(int32_t N, dtc_schedule* out, int max_out);
+/* The same for a given window height and kernel family (split = 1 for the
+ * split-precision forms, whose N-tiles per CTA are capped at 2 at height 32). */
+int dtc_schedule_candidates_ex(int32_t N, int32_t block_h, int split, dtc_schedule* out,
+                               int max_out);
 
 /* Workspace that every candidate's balance mode fits in. */
 dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
-                                        size_t* bytes);
+                                        int32_t block_h, size_t* bytes);
 
 /* Times every candidate (one untimed run + `reps` runs between CUDA events on
  * `stream`; synchronises it) on the given ME-TCF arrays and B form, writes the
@@ -277,7 +283,7 @@ dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, i
 dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                         const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                         const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                        int64_t num_blocks, int bformat, const void* d_Bplane0,
+                        int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
                         const void* d_Bplane1, int32_t N, int precision, float* d_C,
                         void* d_workspace, size_t workspace_bytes, int reps,
                         dtc_schedule* results, int max_results, int* num_results, int* best,
