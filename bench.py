@@ -6,9 +6,14 @@ removed, GCN-normalised values; B = 2^20 x 128 fp32 N(0,1); seeded synthetic
 data standing in for the reference's graph datasets.
 
 One step = one SpMM C = A * B over the whole matrix with A's ME-TCF arrays and
-B already resident in HBM (`value`, GFLOP/s = 2 * nnz * N / t). `e2e` runs the
-reference-facing call (DTCSpMM.run_DTCSpMM) with B in pinned host memory and
-copies C back to the host inside the timed region.
+B already resident in HBM (`value`, GFLOP/s = 2 * nnz * N / t), in the
+split-precision form (SPLIT24 B, relative error <= 1e-5) with the schedule the
+learned cost model picks (window height, mode, waves, N-tiles, form, TCA
+reorder). Beside it: the plain TF32 drop-in with its autotuned schedule (the
+speed-up reference), the exhaustive autotuner's best split schedule, fixed
+schedules of every B form, and the host CSR SpMM. `e2e` runs the
+reference-facing calls (DTCSpMM.pack_b + DTCSpMM.run_DTCSpMM_ex) with B in
+pinned host memory and copies C back to the host inside the timed region.
 
   python bench.py [--gpus N --steps K --warmup W]     # our kernels
   python bench.py --impl reference                    # host CSR SpMM (CPU arm)
@@ -58,6 +63,19 @@ def make_workload(args):
         name = f"uniform-4096-poisson8-N{N}"
     B = gen.normal(A.K, N, seed=1)
     return A, B, N, name
+
+
+def measured_traffic(workload, kernel):
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+    `kernel` on `workload` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic_%s.md" % workload)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = [x.strip() for x in line.strip().strip("|").split("|")]
+        if len(f) >= 2 and f[0] == kernel and f[1].isdigit():
+            return int(f[1])
+    return None
 
 
 def algorithmic_bytes(m, N, b_elem_bytes, with_values=True):
@@ -346,37 +364,89 @@ def main():
         results[k] = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9,
                       "hbm_frac": nbytes / (float(np.mean(per)) * 1e-3) / 1e9 / peaks["hbm_gbs"],
                       "bytes_per_B_elem": eb}
-    tf32_best = min(("tf32_window", "tf32_balance"), key=lambda k: results[k]["ms"])
-    tuned = min(("split24x4_window", "split24x4_balance"), key=lambda k: results[k]["ms"])
+    # autotuned schedules: every (mode, waves, N-tile) at window heights 16 and 32 for the
+    # plain TF32 drop-in and for the two B forms within 1e-5 (dtc_autotune, CUDA events)
+    from dtc_b200 import tune, costmodel, reorder as reorder_mod
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mets = {16: m, 32: metcf.convert(A.rowptr, A.col, A.M, H=32, values=A.val, device=dev)}
+    tuned_tbl = {}
+    for H, mm in mets.items():
+        ws_t = tune.workspace_for(mm, N, dev)
+        for fo in ("tf32", "split24x4", "split24x3"):
+            fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
+            pl = [B] if fo == "tf32" else planes[fmt]
+            scheds, best = tune.autotune(mm, pl, fmt, N, prec, reps=3, out=out_for("tune"),
+                                         workspace=ws_t)
+            tuned_tbl[(fo, H)] = best
+        del ws_t
+    plain_key = min((k for k in tuned_tbl if k[0] == "tf32"), key=lambda k: tuned_tbl[k].ms)
+    exh_key = min((k for k in tuned_tbl if k[0] != "tf32"), key=lambda k: tuned_tbl[k].ms)
+    plain_ms = tuned_tbl[plain_key].ms
 
-    # headline timed region: K steps of the tuned form, clocks sampled
+    # the learned scheduler's choice (features -> MLP on the GPU); the exhaustive
+    # autotuner is its fallback when no weights match the class space
+    t0 = time.perf_counter()
+    plan = costmodel.Scheduler(device=dev).plan(torch.from_numpy(A.rowptr).to(dev),
+                                                torch.from_numpy(A.col).to(dev), m, N, B=B)
+    plan_s = time.perf_counter() - t0
+    perm = None
+    At = A
+    if plan.reorder:
+        t0 = time.perf_counter()
+        perm, rp2, c2, v2 = reorder_mod.reorder(torch.from_numpy(A.rowptr).to(dev),
+                                                torch.from_numpy(A.col).to(dev),
+                                                torch.from_numpy(A.val).to(dev), A.M)
+        torch.cuda.synchronize()
+        tca_s = time.perf_counter() - t0
+        mt = metcf.convert(rp2, c2, A.M, H=plan.H, values=v2, device=dev)
+        At = type("CSR", (), dict(rowptr=rp2.cpu().numpy(), col=c2.cpu().numpy(),
+                                  val=v2.cpu().numpy(), M=A.M, K=A.K, nnz=A.nnz))
+        Bt = B.index_select(0, perm.long()).contiguous()
+    else:
+        tca_s = 0.0
+        mt = mets[plan.H]
+        Bt = B
+    fmt_t, prec_t = tune.FORMS[plan.form][0], tune.FORMS[plan.form][1]
+    planes_t = metcf.pack_b(Bt, fmt_t)
+    sched = tune.Schedule(mode=plan.mode, waves=plan.waves, ntile=plan.ntile,
+                          grid=min(plan.waves * sms, max(mt.T, 1)), ms=0.0)
+    ws_m = tune.workspace_for(mt, N, dev)
+    out_t = out_for("tuned")
+    tuned_fn = lambda: tune.run(mt, planes_t, fmt_t, N, prec_t, sched, out=out_t, workspace=ws_m)
+    tuned = f"{plan.form}_h{plan.H}_mode{plan.mode}_w{plan.waves}_nt{plan.ntile}" + \
+        ("_tca" if plan.reorder else "")
+
+    # headline timed region: K steps of the model-scheduled split form, clocks sampled
     with Clocks(local) as clk:
-        ms, per, wall = timed(forms[tuned][0], args.steps, args.warmup)
+        ms, per, wall = timed(tuned_fn, args.steps, args.warmup)
     clocks = clk.summary()
     value = world * flops / (ms * 1e-3) / 1e9
 
-    nbytes, U, S = algorithmic_bytes(m, N, forms[tuned][1])
+    nbytes, U, S = algorithmic_bytes(mt, N, tune.FORMS[plan.form][2])
     kern_ms = float(np.mean(per))
     achieved = nbytes / (kern_ms * 1e-3) / 1e9
+    traffic = measured_traffic(name, tuned)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                 "peak_kind": peak_kind, "algorithmic_bytes": nbytes, "distinct_rows_U": U,
                 "metcf_bytes": S, "compulsory_bytes": S + A.K * N * 3 + A.M * N * 4,
                 "kernel": tuned, "kernel_ms": kern_ms}
 
     # end-to-end through the public API with host buffers: pinned fp32 B ->
-    # device, storage-form pack, SpMM, C -> pinned host
+    # device (row gather when reordered), storage-form pack, SpMM, C -> pinned host
     Bpin = torch.from_numpy(Bh).pin_memory()
     Cpin = torch.empty((A.M, N), dtype=torch.float32).pin_memory()
     Bdev = torch.empty_like(B)
+    perm_l = None if perm is None else perm.long()
 
     def e2e_step():
         Bdev.copy_(Bpin, non_blocking=True)
-        pl = DTCSpMM.pack_b(Bdev, B_SPLIT24)
-        C = DTCSpMM.run_DTCSpMM_ex(pl, B_SPLIT24, N, m.RowWindowOffset, m.TCblocktileId,
-                                   m.TCblockoffset, m.SparseAToX, A.M, PREC_SPLIT4,
-                                   1 if tuned.endswith("balance") else 0, 0,
-                                   values=m.TCvalues)[0]
+        Bu = Bdev if perm_l is None else Bdev.index_select(0, perm_l)
+        pl = DTCSpMM.pack_b(Bu, fmt_t)
+        C = DTCSpMM.run_DTCSpMM_ex(pl, fmt_t, N, mt.RowWindowOffset, mt.TCblocktileId,
+                                   mt.TCblockoffset, mt.SparseAToX, A.M, prec_t, sched.mode,
+                                   sched.grid, values=mt.TCvalues, ntile=sched.ntile,
+                                   block_h=plan.H)[0]
         Cpin.copy_(C, non_blocking=True)
 
     e2e_steps = max(3, min(args.steps, 10))
@@ -384,16 +454,31 @@ def main():
     e2e = {"value": world * flops / (e_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
            "h2d_bytes_per_step": int(Bh.nbytes), "d2h_bytes_per_step": int(A.M * N * 4),
            "api": "DTCSpMM.pack_b + DTCSpMM.run_DTCSpMM_ex"}
+    learned = {"class": costmodel.CLASSES[plan.cls], "source": plan.source,
+               "plan_s": plan_s, "tca_reorder_s": tca_s, "T": mt.T, "ms": kern_ms,
+               "exhaustive_no_reorder": {"form": exh_key[0], "H": exh_key[1],
+                                         "mode": tuned_tbl[exh_key].mode,
+                                         "waves": tuned_tbl[exh_key].waves,
+                                         "ntile": tuned_tbl[exh_key].ntile,
+                                         "ms": tuned_tbl[exh_key].ms},
+               "plain_tf32_tuned": {"H": plain_key[1], "mode": tuned_tbl[plain_key].mode,
+                                    "waves": tuned_tbl[plain_key].waves,
+                                    "ntile": tuned_tbl[plain_key].ntile, "ms": plain_ms},
+               "autotune": {f"{k[0]}_h{k[1]}": v.ms for k, v in tuned_tbl.items()}}
+    tf32_best = min(("tf32_window", "tf32_balance"), key=lambda k: results[k]["ms"])
 
     cpu, errs = (None, {})
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu, _ = cpu_baseline(A, Bh, N)
-        for k in (tf32_best, tuned, "split24x3_balance", "bf16_balance", "fp8_balance"):
+        for k in (tf32_best, "split24x3_balance", "bf16_balance", "fp8_balance"):
             forms[k][0]()
             torch.cuda.synchronize()
             errs[k] = accuracy_vs_fp64(A, Bh, N, outs[k].cpu().numpy())
             results[k]["rel_err_vs_fp64"] = errs[k]["rel_fro"]
             results[k]["max_abs_err"] = errs[k]["max_abs"]
+        tuned_fn()
+        torch.cuda.synchronize()
+        errs[tuned] = accuracy_vs_fp64(At, Bt.cpu().numpy(), N, out_t.cpu().numpy())
 
     if rank == 0:
         line = {"metric": "SpMM GFLOP/s (2*nnz*N) & HBM-roofline %", "value": value,
@@ -402,13 +487,15 @@ def main():
                 "vs_baseline": None, "dtype": "bf16x2 (split, fp32 accumulate)",
                 "data": "synthetic",
                 "config": {"workload": name, "num_nodes": A.M, "nnz": A.nnz, "N": N,
-                           "T": m.T, "form": tuned, "plain_form": tf32_best,
+                           "T": mt.T, "form": tuned, "plain_form": "tf32_h%d (autotuned)"
+                           % plain_key[1],
                            "l2": "inputs larger than L2 (B %.0f MiB fp32, ME-TCF %.0f MB); no flush"
                            % (A.K * N * 4 / 2 ** 20, S / 1e6)},
-                "speedup_vs_plain_tf32": results[tf32_best]["ms"] / ms,
-                "forms": results, "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu,
-                "accuracy_vs_fp64": errs.get(tuned), "clocks": clocks,
-                "gpu_launches": forms[tuned][2] * args.steps}
+                "speedup_vs_plain_tf32": plain_ms / ms,
+                "forms": results, "learned_schedule": learned, "roofline": roofline,
+                "e2e": e2e, "cpu_baseline": cpu, "accuracy_vs_fp64": errs.get(tuned),
+                "clocks": clocks,
+                "gpu_launches": (2 if sched.mode == 1 and sched.grid > 1 else 1) * args.steps}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

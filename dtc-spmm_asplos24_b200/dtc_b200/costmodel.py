@@ -6,7 +6,8 @@ The reference fixes its schedule by hand per dataset and N
 
     (window height, compaction width, mode, waves, N-tile, B form, reorder)
 
-with window 16 x width 8 TC blocks, mode 0 (window-scheduled) or 1 (strict
+with row windows of 16 or 32 rows and TC blocks 8 columns wide (the kernels'
+compaction width), mode 0 (window-scheduled) or 1 (strict
 balance; the split threshold is ceil(T / CTAs) blocks), waves in {1,2,4,8,16}
 (CTAs = waves x SMs), N-tiles per CTA in {1,2,4}, the two B forms within
 1e-5 relative error (SPLIT24 with 4- or 3-term products) and TCA reorder off or
@@ -32,41 +33,42 @@ from ._lib import MlpDims, call
 from .metcf import _ptr, _stream
 
 NFEAT = 48
+HEIGHTS = (16, 32)
 WAVES = (1, 2, 4, 8, 16)
 NTILES = (1, 2, 4)
 FORMS = ("split24x4", "split24x3")
-CLASSES = [dict(H=16, W=8, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
-           for ro in (0, 1) for fo in FORMS for mo in (0, 1) for wv in WAVES for nt in NTILES]
+CLASSES = [dict(H=h, W=8, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
+           for ro in (0, 1) for h in HEIGHTS for fo in FORMS for mo in (0, 1) for wv in WAVES
+           for nt in NTILES]
 K = len(CLASSES)
-DEFAULT_CLASS = next(i for i, c in enumerate(CLASSES)
-                     if c["mode"] == 1 and c["waves"] == 16 and c["ntile"] == 1
-                     and c["form"] == "split24x4" and c["reorder"] == 0)
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 DATASET_PATH = os.path.join(DATA_DIR, "costmodel_dataset.npz")
 WEIGHTS_PATH = os.path.join(DATA_DIR, "costmodel_weights.npz")
 
 
-def auto_ntile(N):
-    return 1 if N <= 128 else 2 if N <= 256 else 4
+def auto_ntile(N, H=16):
+    """N-tiles per CTA the split kernels use when uncapped (2 at most at H = 32)."""
+    nt = 1 if N <= 128 else 2 if N <= 256 else 4
+    return min(nt, 2) if H == 32 else nt
 
 
 def feasible(N):
     """uint8 [K]: classes whose N-tile the kernels run for width N."""
-    return np.array([c["ntile"] <= auto_ntile(N) for c in CLASSES], np.uint8)
+    return np.array([c["ntile"] <= auto_ntile(N, c["H"]) for c in CLASSES], np.uint8)
 
 
-def class_of(mode, waves, ntile, form, reorder):
-    for i, c in enumerate(CLASSES):
-        if (c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"]) == \
-                (mode, waves, ntile, form, reorder):
-            return i
-    raise KeyError((mode, waves, ntile, form, reorder))
+_INDEX = {(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"]): i
+          for i, c in enumerate(CLASSES)}
+
+
+def class_of(mode, waves, ntile, form, reorder, H=16):
+    return _INDEX[(mode, waves, ntile, form, reorder, H)]
 
 
 def default_class(N):
-    """The untuned library default for width N (strict balance, 16 waves, all
-    N-tiles in one CTA, SPLIT24 4-term, no reorder)."""
-    return class_of(1, 16, auto_ntile(N), "split24x4", 0)
+    """The untuned library default for width N (window height 16, strict
+    balance, 16 waves, all N-tiles in one CTA, SPLIT24 4-term, no reorder)."""
+    return class_of(1, 16, auto_ntile(N), "split24x4", 0, 16)
 
 
 # ----------------------------------------------------------------- features
@@ -266,24 +268,28 @@ def measure(spec, reps=3, device="cuda"):
     B = torch.from_numpy(gen.normal(A.M, N, seed=spec["seed"] + 2)).to(device)
     times = np.full(K, np.nan, np.float32)
     info = dict(M=A.M, nnz=int(cl.numel()), T0=m.T)
+    out = torch.empty((A.M, N), dtype=torch.float32, device=device)
+    planes = {fo: metcf.pack_b(B, tune.FORMS[fo][0]) for fo in FORMS}
     for ro in (0, 1):
-        mm = m
+        src = (rp, cl, vl)
         if ro:
             t0 = time.perf_counter()
             _, rp2, c2, v2 = reorder_mod.reorder(rp, cl, vl, A.M)
             torch.cuda.synchronize()
             info["tca_s"] = time.perf_counter() - t0
-            mm = metcf.convert(rp2, c2, A.M, values=v2)
-            info["T1"] = mm.T
-        ws = tune.workspace_for(mm, N, B.device)
-        out = torch.empty((A.M, N), dtype=torch.float32, device=device)
-        for fo in FORMS:
-            fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
-            planes = metcf.pack_b(B, fmt)
-            scheds, _ = tune.autotune(mm, planes, fmt, N, prec, reps=reps, out=out, workspace=ws)
-            for s in scheds:
-                times[class_of(s.mode, s.waves, s.ntile, fo, ro)] = s.ms
-        del ws, out
+            src = (rp2, c2, v2)
+        for h in HEIGHTS:
+            mm = m if (h == 16 and not ro) else metcf.convert(src[0], src[1], A.M, H=h,
+                                                              values=src[2])
+            info[f"T_r{ro}_h{h}"] = mm.T
+            ws = tune.workspace_for(mm, N, B.device)
+            for fo in FORMS:
+                fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
+                scheds, _ = tune.autotune(mm, planes[fo], fmt, N, prec, reps=reps, out=out,
+                                          workspace=ws)
+                for s in scheds:
+                    times[class_of(s.mode, s.waves, s.ntile, fo, ro, h)] = s.ms
+            del ws, mm
     return feat, times, info
 
 
@@ -338,6 +344,7 @@ def fit(ds, steps=3000, lr=2e-3, seed=0, device="cuda"):
 @dataclass
 class Plan:
     cls: int
+    H: int
     form: str
     reorder: bool
     mode: int
@@ -348,10 +355,13 @@ class Plan:
 
 class Scheduler:
     """Picks a class for (matrix, N): the trained model when its weights are
-    present, else the exhaustive autotuner over every class."""
+    present and match the class space, else the exhaustive autotuner over every
+    class."""
 
     def __init__(self, weights=WEIGHTS_PATH, device="cuda"):
         self.net = MLP.load(weights, device) if weights and os.path.exists(weights) else None
+        if self.net is not None and self.net.dims != (NFEAT, 64, 64, K):
+            self.net = None  # weights of another class space: fall back
 
     def plan(self, rowptr, col, m: metcf.METCF, N, exhaustive=False, B=None, reps=3):
         if self.net is not None and not exhaustive:
@@ -362,7 +372,8 @@ class Scheduler:
             c = self._exhaustive(rowptr, col, m, N, B, reps)
             src = "exhaustive"
         k = CLASSES[c]
-        return Plan(c, k["form"], bool(k["reorder"]), k["mode"], k["waves"], k["ntile"], src)
+        return Plan(c, k["H"], k["form"], bool(k["reorder"]), k["mode"], k["waves"], k["ntile"],
+                    src)
 
     @staticmethod
     def _exhaustive(rowptr, col, m, N, B, reps):
@@ -371,15 +382,17 @@ class Scheduler:
             B = torch.randn((m.M, N), device=dev)
         best, best_c = None, None
         for ro in (0, 1):
-            mm = m
+            src = (rowptr.to(dev), col.to(dev), m.TCvalues)
             if ro:
-                _, rp2, c2, v2 = reorder_mod.reorder(rowptr.to(dev), col.to(dev), None, m.M)
-                mm = metcf.convert(rp2, c2, m.M, values=v2)
-            for fo in FORMS:
-                fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
-                scheds, b = tune.autotune(mm, metcf.pack_b(B, fmt), fmt, N, prec, reps=reps)
-                if best is None or b.ms < best:
-                    best, best_c = b.ms, class_of(b.mode, b.waves, b.ntile, fo, ro)
+                _, rp2, c2, _ = reorder_mod.reorder(src[0], src[1], None, m.M)
+                src = (rp2, c2, None)
+            for h in HEIGHTS:
+                mm = m if (h == m.H and not ro) else metcf.convert(src[0], src[1], m.M, H=h)
+                for fo in FORMS:
+                    fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
+                    scheds, b = tune.autotune(mm, metcf.pack_b(B, fmt), fmt, N, prec, reps=reps)
+                    if best is None or b.ms < best:
+                        best, best_c = b.ms, class_of(b.mode, b.waves, b.ntile, fo, ro, h)
         return best_c
 
 

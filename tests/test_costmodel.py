@@ -43,12 +43,16 @@ def test_oracle_gradients_match_finite_differences():
 
 
 def test_class_space():
-    assert cm.K == 2 * 2 * 2 * 5 * 3
+    assert cm.K == 2 * 2 * 2 * 2 * 5 * 3  # reorder x height x form x mode x waves x N-tile
     assert cm.feasible(128).sum() == cm.K // 3
-    assert cm.feasible(512).sum() == cm.K
+    # at window height 32 the split kernels hold at most 2 N-tiles per CTA
+    assert cm.feasible(512).sum() == cm.K // 2 + cm.K // 3
     d = cm.CLASSES[cm.default_class(512)]
-    assert (d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == (1, 16, 4, "split24x4", 0)
-    assert all(c["H"] == 16 and c["W"] == 8 for c in cm.CLASSES)
+    assert (d["H"], d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == \
+        (16, 1, 16, 4, "split24x4", 0)
+    assert {c["H"] for c in cm.CLASSES} == {16, 32} and all(c["W"] == 8 for c in cm.CLASSES)
+    assert len({cm.class_of(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"])
+                for c in cm.CLASSES}) == cm.K
 
 
 def test_targets_and_regret():
