@@ -2,6 +2,7 @@
 // argument checks, status/error text, per-device state, dispatch.
 #include <mutex>
 #include <string>
+#include <cudaTypedefs.h>
 #include "impl.h"
 
 namespace dtc {
@@ -50,6 +51,39 @@ bool is_sm100() {
   std::lock_guard<std::mutex> lk(g_mu);
   fill_dev_props(d);
   return g_major[d] == 10;
+}
+
+dtc_status encode_c_map(CUtensorMap* map, float* C, int64_t M, int32_t N, int box_rows) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  static std::once_flag once;
+  static cudaError_t lookup = cudaSuccess;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    lookup = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (lookup == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fn);
+  });
+  if (!encode) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return DTC_ERR_UNSUPPORTED;
+  }
+  if (((uintptr_t)C & 15) != 0 || N % 4 != 0 || M < 1 || N < 1) {
+    set_error("C must be 16-byte aligned with N % 4 == 0");
+    return DTC_ERR_INVALID_ARGUMENT;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)M};
+  const cuuint64_t strides[1] = {(cuuint64_t)N * sizeof(float)};
+  const cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for C (code " + std::to_string((int)r) + ")");
+    return DTC_ERR_CUDA;
+  }
+  return DTC_OK;
 }
 
 uint32_t* device_error_word() {

@@ -110,6 +110,42 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Bulk (TMA engine) store of `bytes` (multiple of 16, both addresses 16-byte
+// aligned) from shared to global memory, tracked by this thread's bulk group.
+__device__ __forceinline__ void bulk_store_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst),
+               "r"(smem_u32(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Waits until at most one (N = 1) / no (N = 0) committed group still reads its
+// shared-memory source.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// TMA 2-D tile store: the box at (x, y) of `map` from shared memory `ssrc`
+// (128-byte aligned), tracked by this thread's bulk group. Parts of the box
+// outside the tensor are not written. x * element size must be a multiple of
+// 16 bytes and x, y must not be negative.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* ssrc, int32_t x,
+                                             int32_t y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+               ::"l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(ssrc)), "r"(x), "r"(y)
+               : "memory");
+}
+
+// Waits until every committed group has completed (writes performed).
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+// Barrier over `count` threads (multiple of 32) on hardware barrier `id` (1-15).
+__device__ __forceinline__ void named_bar_sync(uint32_t id, uint32_t count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
 // TMA 2-D tile::gather4: four rows (r0..r3) of `box` width starting at column
 // `x` (x * element size must be a multiple of 16 bytes) into consecutive
 // 128-byte smem rows at `dst`; completes `bytes` on `bar`. Rows outside the

@@ -22,6 +22,10 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
                            cudaStream_t st, int ntile = 0, Epilogue epi = {}, int H = 16);
+// Tensor map of the row-major fp32 matrix C [M x N] with boxes of 32 columns x
+// `box_rows` rows, for TMA stores of finished row-window tiles. Needs C
+// 16-byte aligned and N % 4 == 0.
+dtc_status encode_c_map(CUtensorMap* map, float* C, int64_t M, int32_t N, int box_rows);
 size_t spmm_partials_bytes(int64_t T, int32_t N, int grid, int H = 16);
 dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* rwo,
                         cudaStream_t st);

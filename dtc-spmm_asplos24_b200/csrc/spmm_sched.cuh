@@ -15,6 +15,7 @@ inline int default_grid() { return kWavesPerSm * num_sms(); }
 constexpr int kBlkW = 8;        // TC-block width (BLK_W)
 
 struct Params {
+  CUtensorMap cmap;          // C [M x N] fp32, box 32 columns x window height (TMA stores)
   const int32_t* rwo;        // RowWindowOffset [nwin+1]
   const uint8_t* tile;       // TCblocktileId [nnz]
   const int32_t* toff;       // TCblockoffset [T+1]

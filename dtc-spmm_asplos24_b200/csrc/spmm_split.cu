@@ -69,7 +69,9 @@ struct SCfg {
   static constexpr int kE = S * kStageE;
   static constexpr int kY = S * kStageY;
   static constexpr int kBars = (3 * S + 2 * kNacc) * 8;
-  static constexpr int kSmem = kX + kE + kY + kBars + 16 + 1024;
+  static constexpr int kStgW = 16 * 32 * 4;          // one epilogue warp's 16-row C tile
+  static constexpr int kStg = kEpiWarps * 2 * kStgW;  // double-buffered per warp
+  static constexpr int kSmem = kX + kE + kY + kStg + kBars + 16 + 1024;
   static constexpr int kCols = kMmaWarps * kNacc * kAccCols;
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
@@ -96,14 +98,15 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
 }
 
 template <int FORM, int NT, int P, int S, bool FOUR, int WH>
-__global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
+__global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constant__ Params p) {
   using K = SCfg<FORM, NT, P, S, WH>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* xring = smem;
   uint8_t* ering = smem + K::kX;
   uint8_t* yring = ering + K::kE;
-  uint64_t* bars = (uint64_t*)(yring + K::kY);
+  uint8_t* stg = yring + K::kY;  // [4 warps][2][16 x 32] fp32 C staging
+  uint64_t* bars = (uint64_t*)(stg + K::kStg);
   uint64_t* loaded = bars;               // [S] 32 cp.async arrivals
   uint64_t* full = bars + S;             // [S] 1 tile-builder + 1 converter arrival
   uint64_t* empty = bars + 2 * S;        // [S] UMMA commit
@@ -252,11 +255,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       const int64_t sb = b0 + st * P;
       return (st < nstage && lane <= P && sb + lane <= b1) ? __ldg(p.toff + sb + lane) : 0;
     };
+    // Tile ids and values of the first 64 entries of a stage are loaded one
+    // owned stage ahead (offsets two ahead), so their global-load latency
+    // overlaps the previous stage's work instead of stalling this one.
     int32_t offv = offs_of(tw);
+    int32_t offn = offs_of(tw + kTileWarps);
+    uint32_t pt0 = 0, pt1 = 0;
+    float pv0 = 0.0f, pv1 = 0.0f;
+    auto fetch = [&](int64_t st, int32_t ov) {
+      const int64_t sb = b0 + st * P;
+      const int nbx = st < nstage ? (int)((b1 - sb) < P ? (b1 - sb) : P) : 0;
+      const int32_t f0 = __shfl_sync(0xffffffffu, ov, 0), f1 = __shfl_sync(0xffffffffu, ov, nbx);
+      const int32_t e = f0 + lane;
+      pt0 = (e < f1) ? __ldg(p.tile + e) : 0u;
+      pv0 = (e < f1) ? (p.vals ? __ldg(p.vals + e) : 1.0f) : 0.0f;
+      pt1 = (e + 32 < f1) ? __ldg(p.tile + e + 32) : 0u;
+      pv1 = (e + 32 < f1) ? (p.vals ? __ldg(p.vals + e + 32) : 1.0f) : 0.0f;
+    };
+    fetch(tw, offv);
     for (int64_t st = tw; st < nstage; st += kTileWarps) {
       const int s = (int)(st % S);
       const uint32_t n = (uint32_t)(st / S);
-      const int32_t nxt = offs_of(st + kTileWarps);
+      const int32_t nxt = offs_of(st + 2 * kTileWarps);
+      const uint32_t ct0 = pt0, ct1 = pt1;
+      const float cv0 = pv0, cv1 = pv1;
+      fetch(st + kTileWarps, offn);
       const int64_t sb = b0 + st * P;
       const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
       int32_t off[P + 1];
@@ -273,8 +296,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
         int pb = 0;
 #pragma unroll
         for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
-        const uint32_t pos = __ldg(p.tile + e);
-        const float v = p.vals ? __ldg(p.vals + e) : 1.0f;
+        const int32_t i = (e - e0) >> 5;  // chunk of this entry
+        const uint32_t pos = i == 0 ? ct0 : i == 1 ? ct1 : __ldg(p.tile + e);
+        const float v = i == 0 ? cv0 : i == 1 ? cv1 : (p.vals ? __ldg(p.vals + e) : 1.0f);
         if (pos >= WH * kBlkW) {
           atomicOr(p.err, kErrBadIndex);
           continue;
@@ -293,7 +317,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&full[s]);
-      offv = nxt;
+      offv = offn;
+      offn = nxt;
     }
   } else if (warp >= kConvWarp0) {
     // --------------------------------------------------------- converters
@@ -479,6 +504,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
     cta_windows(p, c, b0, b1, ws, we);
     const int ew = warp;
     uint32_t q = 0;
+    uint32_t su = 0;  // C tiles this warp has staged (selects the staging buffer)
     int64_t rn0 = ws < we ? __ldg(p.rwo + ws) : 0;
     int64_t rn1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
     for (int32_t w = ws; w < we; ++w) {
@@ -536,18 +562,33 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const Params p) {
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[a]);
           }
-          if (f < p.N) {
-            float* o = out + (size_t)h * 16 * p.N;
-            const int64_t rb = row0 + h * 16;
+          if (!guard_rows) {  // partial tile of a cut window: raw sums to the workspace
+            if (f < p.N) {
+              float* o = out + (size_t)h * 16 * p.N;
 #pragma unroll
-            for (int r = 0; r < 16; ++r)
-              if (!guard_rows) o[r * p.N + f] = x[r];  // partial tile: raw sum
-              else if (rb + r < p.M) o[r * p.N + f] = epilogue(p, x[r], f);
+              for (int r = 0; r < 16; ++r) o[r * p.N + f] = x[r];
+            }
+          } else if (col0 + t * 128 + ew * 32 < p.N) {
+            // finished 16-row tile of this warp's 32 columns: shared memory, then
+            // one TMA store (rows past M and columns past N are clipped)
+            float* sb = reinterpret_cast<float*>(stg + (ew * 2 + (su & 1)) * K::kStgW);
+            __syncwarp();  // lane 0 has waited for this buffer's previous store
+#pragma unroll
+            for (int r = 0; r < 16; ++r) sb[r * 32 + lane] = epilogue(p, x[r], f < p.N ? f : 0);
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+              tma_store_2d(&p.cmap, sb, col0 + t * 128 + ew * 32, (int32_t)(row0 + h * 16));
+              bulk_commit();
+              bulk_wait_read<1>();
+            }
+            ++su;
           }
         }
       }
       ++q;
     }
+    if (lane == 0) bulk_wait_all();
   }
 
   tc_fence_before();
@@ -586,8 +627,8 @@ template <int FORM, bool FOUR>
 dtc_status dispatch_n(const Params& p, cudaStream_t st, int ntile) {
   int nt = p.N <= 128 ? 1 : p.N <= 256 ? 2 : 4;
   if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
-  if (p.H == 32) {
-    if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
+  if (p.H == 32) {  // 3 blocks per stage keep the 32-row A tiles within shared memory
+    if (nt == 1) return launch_split<FORM, 1, 3, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
     return launch_split<FORM, 2, 2, 8, FOUR, 32>(p, (p.N + 255) / 256, st);
   }
   if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 16>(p, (p.N + 127) / 128, st);
@@ -628,6 +669,9 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   p.C = C; p.part = part; p.err = device_error_word();
   p.bias = epi.bias; p.relu = epi.relu;
   p.M = M; p.nwin = nwin; p.N = N; p.T = T; p.mode = mode; p.H = H;
+  DTC_REQUIRE(((uintptr_t)C & 15) == 0, "C must be 16-byte aligned");
+  dtc_status es = encode_c_map(&p.cmap, C, M, N, 16);
+  if (es != DTC_OK) return es;
   int G = grid > 0 ? grid : default_grid();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;

@@ -39,6 +39,10 @@ def test_reference_kernels_agree(cuda, tmp_path):
     ref = O.spmm_f64(A.rowptr, A.col, ones, A.M, B)
     bound = O.spmm_absbound_f64(A.rowptr, A.col, ones, A.M, B)
     assert int(res["device_status"]) == 0
+    # the reference's balance entry zero-fills C once per call and then runs its
+    # 1000 timing launches, each adding its partial rows with atomicAdd
+    # (DTCSpMM_kernel.cu:1130, :1141-1180): its C holds 1000 x the product
+    res["ref_balance_float4_split_C"] = res["ref_balance_float4_split_C"] / 1000.0
     for k in ("ref_window_float_nonsplit_C", "ref_window_float4_split_C",
               "ref_balance_float4_split_C", "ours_window_C", "ours_balance_C"):
         err = np.abs(res[k].astype(np.float64) - ref)
