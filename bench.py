@@ -65,16 +65,20 @@ def make_workload(args):
     return A, B, N, name
 
 
+TRAFFIC_FILES = {"rmat-2^20-sym-gcn-N128": "dram_traffic_rmat20_N128.md"}
+
+
 def measured_traffic(workload, kernel):
     """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
     `kernel` on `workload` from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "traffic_%s.md" % workload)
-    if not os.path.exists(p):
+    f = TRAFFIC_FILES.get(workload)
+    p = os.path.join(ROOT, "profiles", f) if f else None
+    if not p or not os.path.exists(p):
         return None
     for line in open(p):
-        f = [x.strip() for x in line.strip().strip("|").split("|")]
-        if len(f) >= 2 and f[0] == kernel and f[1].isdigit():
-            return int(f[1])
+        cells = [x.strip().strip("`") for x in line.strip().strip("|").split("|")]
+        if len(cells) >= 2 and cells[0] == kernel and cells[1].replace(",", "").isdigit():
+            return int(cells[1].replace(",", ""))
     return None
 
 

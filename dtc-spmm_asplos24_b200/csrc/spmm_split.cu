@@ -23,9 +23,9 @@
 // gathering 3 (SPLIT24), 2 (BF16) or 1 (FP8) bytes per element instead of 4.
 //
 // Schedule, work split and the deterministic reduction are the tf32
-// kernel's (spmm_tc.cu). Warp roles (768 threads): epilogue 0-3, UMMA
-// issuers 4-5, loaders 6-7 (cp.async of the planes), tile builders 8-15
-// (A_hi / A_lo tiles), converters 16-23 (wait for a stage's gathered rows,
+// kernel's (spmm_tc.cu). Warp roles (704 threads): epilogue 0-3, UMMA
+// issuers 4-5, loaders 6-9 (cp.async of the planes), tile builders 10-13
+// (A_hi / A_lo tiles), converters 14-21 (wait for a stage's gathered rows,
 // rebuild the bf16 operand rows in place). A stage is released to the UMMA
 // issuers by one tile-builder and one converter arrival.
 #include <cuda_bf16.h>
@@ -39,13 +39,13 @@ namespace {
 constexpr int kEpiWarps = 4;     // warps 0-3
 constexpr int kMmaWarp = 4;      // warps 4-5
 constexpr int kMmaWarps = 2;
-constexpr int kLoadWarp0 = kMmaWarp + kMmaWarps;   // warps 6-7
-constexpr int kLoadWarps = 2;
-constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;  // warps 8-15
-constexpr int kTileWarps = 8;
-constexpr int kConvWarp0 = kTileWarp0 + kTileWarps;  // warps 16-23
+constexpr int kLoadWarp0 = kMmaWarp + kMmaWarps;   // warps 6-9
+constexpr int kLoadWarps = 4;
+constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;  // warps 10-13
+constexpr int kTileWarps = 4;
+constexpr int kConvWarp0 = kTileWarp0 + kTileWarps;  // warps 14-21
 constexpr int kConvWarps = 8;
-constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 768
+constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 704
 constexpr int kTileBytes = 4096;  // per block and 128-feature tile: 16 K rows x 128 bf16
 
 enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2 };
