@@ -297,7 +297,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from dtc_b200 import metcf, B_F32, B_SPLIT24, B_BF16, B_FP8, PREC_TF32, PREC_SPLIT3, PREC_SPLIT4
+    from dtc_b200 import metcf, replicas, B_F32, B_SPLIT24, B_BF16, B_FP8, PREC_TF32, PREC_SPLIT3, PREC_SPLIT4
     import DTCSpMM
 
     A, Bh, N, name = make_workload(args)
@@ -354,11 +354,7 @@ def main():
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         per = [a.elapsed_time(b) for a, b in evs]
-        total = float(e0.elapsed_time(e1))
-        if dist:
-            t = torch.tensor([total], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = replicas.max_over_ranks(float(e0.elapsed_time(e1)), dist, dev)
         return total / steps, per, wall
 
     results = {}
@@ -424,7 +420,7 @@ def main():
     with Clocks(local) as clk:
         ms, per, wall = timed(tuned_fn, args.steps, args.warmup)
     clocks = clk.summary()
-    value = world * flops / (ms * 1e-3) / 1e9
+    value = replicas.aggregate_gflops(flops, ms, world)
 
     nbytes, U, S = algorithmic_bytes(mt, N, tune.FORMS[plan.form][2])
     kern_ms = float(np.mean(per))
