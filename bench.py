@@ -271,7 +271,7 @@ def run_batched(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="rmat", choices=["rmat", "stencil", "uniform", "batched"])
@@ -383,11 +383,13 @@ def main():
     exh_key = min((k for k in tuned_tbl if k[0] != "tf32"), key=lambda k: tuned_tbl[k].ms)
     plain_ms = tuned_tbl[plain_key].ms
 
-    # the learned scheduler's choice (features -> MLP on the GPU); the exhaustive
-    # autotuner is its fallback when no weights match the class space
+    # the learned scheduler's choice (features -> MLP on the GPU, its 4 cheapest
+    # predicted classes timed on this matrix); the exhaustive autotuner is its
+    # fallback when no weights match the class space
     t0 = time.perf_counter()
     plan = costmodel.Scheduler(device=dev).plan(torch.from_numpy(A.rowptr).to(dev),
-                                                torch.from_numpy(A.col).to(dev), m, N, B=B)
+                                                torch.from_numpy(A.col).to(dev), m, N, B=B,
+                                                verify_top=4)
     plan_s = time.perf_counter() - t0
     perm = None
     At = A

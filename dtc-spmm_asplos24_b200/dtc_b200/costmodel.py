@@ -196,19 +196,31 @@ def targets(times):
     return y.astype(np.float32), ok.astype(np.float32)
 
 
-def evaluate(choices, times, N):
-    """Regret of chosen classes vs the exhaustive best, next to the default's."""
+def evaluate(choices, times, N, pred=None, topk=4):
+    """Regret of chosen classes vs the exhaustive best, next to the default's.
+    With the model's predictions `pred` [S, K], also the regret of timing its
+    `topk` cheapest predicted classes and keeping the fastest."""
     t = np.asarray(times, np.float64)
     best = np.nanmin(t, axis=1)
     pick = t[np.arange(len(t)), choices]
     dflt = np.array([t[i, default_class(int(n))] for i, n in enumerate(N)])
     reg = pick / best - 1.0
     dreg = dflt / best - 1.0
-    return dict(n=len(t), regret_mean=float(np.mean(reg)), regret_median=float(np.median(reg)),
-                regret_p90=float(np.quantile(reg, 0.9)), default_regret_mean=float(np.mean(dreg)),
-                speedup_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / pick)))),
-                exhaustive_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / best)))),
-                picked_reorder_frac=float(np.mean([CLASSES[c]["reorder"] for c in choices])))
+    out = dict(n=len(t), regret_mean=float(np.mean(reg)), regret_median=float(np.median(reg)),
+               regret_p90=float(np.quantile(reg, 0.9)), default_regret_mean=float(np.mean(dreg)),
+               speedup_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / pick)))),
+               exhaustive_vs_default_geomean=float(np.exp(np.mean(np.log(dflt / best)))),
+               picked_reorder_frac=float(np.mean([CLASSES[c]["reorder"] for c in choices])))
+    if pred is not None:
+        vk = []
+        for i, n in enumerate(N):
+            ok = np.flatnonzero(feasible(int(n)))
+            top = ok[np.argsort(np.asarray(pred[i])[ok], kind="stable")[:topk]]
+            vk.append(np.nanmin(t[i, top]))
+        vk = np.array(vk)
+        out[f"regret_top{topk}_mean"] = float(np.mean(vk / best - 1.0))
+        out[f"regret_top{topk}_median"] = float(np.median(vk / best - 1.0))
+    return out
 
 
 # ------------------------------------------------------- data collection
@@ -337,7 +349,8 @@ def fit(ds, steps=3000, lr=2e-3, seed=0, device="cuda"):
     net.train(ds["features"][tr], y[tr], mk[tr], steps=steps, lr=lr, seed=seed)
     feas = np.stack([feasible(int(n)) for n in N[~tr]])
     ch = net.choose(ds["features"][~tr], feas)
-    return net, evaluate(ch, ds["times"][~tr], N[~tr])
+    _, _, Y = net.forward(ds["features"][~tr])
+    return net, evaluate(ch, ds["times"][~tr], N[~tr], pred=Y.cpu().numpy())
 
 
 # ------------------------------------------------------------- scheduler
@@ -363,17 +376,68 @@ class Scheduler:
         if self.net is not None and self.net.dims != (NFEAT, 64, 64, K):
             self.net = None  # weights of another class space: fall back
 
-    def plan(self, rowptr, col, m: metcf.METCF, N, exhaustive=False, B=None, reps=3):
+    def plan(self, rowptr, col, m: metcf.METCF, N, exhaustive=False, B=None, reps=3,
+             verify_top=0):
+        """The class to run. With verify_top = k > 1 the model's k cheapest
+        predicted classes are timed on the caller's data and the fastest wins
+        (model-guided search: k measurements instead of the exhaustive 240)."""
         if self.net is not None and not exhaustive:
             f = features(rowptr, col, m, N).reshape(1, -1)
-            c = int(self.net.choose(f, feasible(N))[0])
-            src = "model"
+            if verify_top > 1:
+                _, _, Y = self.net.forward(f)
+                y = Y[0].cpu().numpy()
+                ok = np.flatnonzero(feasible(N))
+                top = ok[np.argsort(y[ok], kind="stable")[:verify_top]]
+                c = self._fastest(rowptr, col, m, N, B, reps, [int(i) for i in top])
+                src = "model+verify"
+            else:
+                c = int(self.net.choose(f, feasible(N))[0])
+                src = "model"
         else:
             c = self._exhaustive(rowptr, col, m, N, B, reps)
             src = "exhaustive"
         k = CLASSES[c]
         return Plan(c, k["H"], k["form"], bool(k["reorder"]), k["mode"], k["waves"], k["ntile"],
                     src)
+
+    @staticmethod
+    def _fastest(rowptr, col, m, N, B, reps, classes):
+        """Times the given classes on this matrix (CUDA events) and returns the fastest."""
+        dev = m.RowWindowOffset.device
+        if B is None:
+            B = torch.randn((m.M, N), device=dev)
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mets, perms, best, best_c = {}, {}, None, None
+        out = torch.empty((m.M, N), dtype=torch.float32, device=dev)
+        for c in classes:
+            k = CLASSES[c]
+            key = (k["reorder"], k["H"])
+            if key not in mets:
+                if k["reorder"]:
+                    if "p" not in perms:
+                        perms["p"] = reorder_mod.reorder(rowptr.to(dev), col.to(dev), None, m.M)
+                    _, rp2, c2, _ = perms["p"]
+                    mets[key] = metcf.convert(rp2, c2, m.M, H=k["H"])
+                else:
+                    mets[key] = m if k["H"] == m.H else metcf.convert(rowptr.to(dev),
+                                                                      col.to(dev), m.M, H=k["H"])
+            mm = mets[key]
+            fmt, prec = tune.FORMS[k["form"]][0], tune.FORMS[k["form"]][1]
+            planes = metcf.pack_b(B, fmt)
+            sched = tune.Schedule(mode=k["mode"], waves=k["waves"], ntile=k["ntile"],
+                                  grid=min(k["waves"] * sms, max(mm.T, 1)), ms=0.0)
+            ws = tune.workspace_for(mm, N, dev)
+            tune.run(mm, planes, fmt, N, prec, sched, out=out, workspace=ws)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                tune.run(mm, planes, fmt, N, prec, sched, out=out, workspace=ws)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            if best is None or ms < best:
+                best, best_c = ms, c
+        return best_c
 
     @staticmethod
     def _exhaustive(rowptr, col, m, N, B, reps):

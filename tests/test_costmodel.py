@@ -173,3 +173,26 @@ def test_trained_model_beats_default_on_held_out(cuda):
     assert ev["speedup_vs_default_geomean"] > 1.0, ev
     assert ev["regret_mean"] < ev["default_regret_mean"], ev
     assert ev["regret_median"] < 0.10, ev
+    assert ev["regret_top4_mean"] <= ev["regret_mean"], ev
+
+
+@pytest.mark.gpu
+def test_scheduler_verifies_top_predictions(cuda):
+    """Model-guided search: the plan is the fastest of the model's k cheapest
+    predicted classes, timed on the caller's matrix."""
+    if not os.path.exists(cm.WEIGHTS_PATH):
+        pytest.skip("no trained weights committed")
+    import torch
+    from dtc_b200 import gen, metcf
+    A = gen.zipf(20000, seed=4)
+    rp, col = torch.from_numpy(A.rowptr).cuda(), torch.from_numpy(A.col).cuda()
+    m = metcf.convert(rp, col, A.M, values=torch.from_numpy(A.val).cuda())
+    s = cm.Scheduler()
+    plain = s.plan(rp, col, m, 128)
+    ver = s.plan(rp, col, m, 128, verify_top=3)
+    assert plain.source == "model" and ver.source == "model+verify"
+    _, _, Y = s.net.forward(cm.features(rp, col, m, 128).reshape(1, -1))
+    y = Y[0].cpu().numpy()
+    ok = np.flatnonzero(cm.feasible(128))
+    top = set(ok[np.argsort(y[ok], kind="stable")[:3]].tolist())
+    assert plain.cls in top and ver.cls in top
