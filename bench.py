@@ -248,6 +248,9 @@ def run_batched(args):
 
     bs = batched.BatchedSpMM(mats, N)
     bs.load(Bt)
+    t0 = time.perf_counter()
+    table = bs.autotune(reps=3)
+    tune_s = time.perf_counter() - t0
     bs.capture()
     one_ms = timed(bs.run, args.steps, args.warmup)
     ms_sep, run_sep = batched.separate_launches(mats, N)
@@ -263,7 +266,11 @@ def run_batched(args):
                        "rows": int(sum(m.M for m in mats)), "T": bs.m.T},
             "separate_launches_ms": sep_ms,
             "separate_launches_gflops": flops / (sep_ms * 1e-3) / 1e9,
-            "speedup_vs_separate": sep_ms / one_ms, "gpu_launches": 2 * args.steps,
+            "speedup_vs_separate": sep_ms / one_ms,
+            "gpu_launches": (2 if bs.mode == 1 and bs.grid > 1 else 1) * args.steps,
+            "schedule": {"H": bs.m.H, "mode": bs.mode, "grid": bs.grid, "ntile": bs.ntile,
+                         "autotune_ms": {h: v.ms for h, v in table.items()},
+                         "autotune_s": tune_s},
             "generation_s": gen_s}
     print(json.dumps(line), flush=True)
 

@@ -78,7 +78,8 @@ class BatchedSpMM:
         self.device = torch.device(device)
         self.fmt = B_F32 if fmt is None else fmt
         self.precision = PREC_TF32 if precision is None else precision
-        self.mode, self.grid = mode, grid
+        self.mode, self.grid, self.ntile = mode, grid, 0
+        self._csr = (rowptr, col, val)
         self.m = _m.convert(rowptr, col, self.layout.total_rows, values=val, device=self.device)
         self.B = torch.zeros((self.layout.total_rows, N), dtype=torch.float32, device=self.device)
         self.C = torch.empty((self.layout.total_rows, N), dtype=torch.float32, device=self.device)
@@ -86,6 +87,32 @@ class BatchedSpMM:
         self.ws = torch.empty(max(_m.spmm_balance_workspace_bytes(self.m, N), 1),
                               dtype=torch.uint8, device=self.device)
         self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+    def autotune(self, heights=(16, 32), reps=3):
+        """Exhaustive schedule search for this batch (dtc_autotune): window height
+        (16 or 32; a 32-row window may span two stacked matrices, which only adds
+        distinct columns to it), strict balance or window mode, the CTA count
+        (which sets the split threshold, blocks per CTA) and the N-tiles per CTA.
+        Keeps the fastest and returns {height: best Schedule}."""
+        from . import tune
+        from ._lib import B_F32
+        best, table = None, {}
+        for h in heights:
+            mm = self.m if h == self.m.H else _m.convert(*self._csr[:2], self.layout.total_rows,
+                                                          H=h, values=self._csr[2],
+                                                          device=self.device)
+            planes = [self.B] if self.fmt == B_F32 else _m.pack_b(self.B, self.fmt)
+            _, b = tune.autotune(mm, planes, self.fmt, self.N, self.precision, reps=reps,
+                                 out=self.C)
+            table[h] = b
+            if best is None or b.ms < best[1].ms:
+                best = (mm, b)
+        self.m, sched = best
+        self.mode, self.grid, self.ntile = sched.mode, sched.grid, sched.ntile
+        self.ws = torch.empty(max(tune.workspace_for(self.m, self.N, self.device).numel(), 1),
+                              dtype=torch.uint8, device=self.device)
+        self.graph = None
+        return table
 
     def load(self, Bs: List[torch.Tensor]):
         """Copy per-matrix operands into the stacked operand (rows beyond each
@@ -103,7 +130,7 @@ class BatchedSpMM:
                 self.planes = _m.pack_b(self.B, self.fmt)
             planes = _m.pack_b_into(self.B, self.fmt, self.planes)
         _m.spmm_ex(self.m, planes, self.fmt, self.N, self.precision, mode=self.mode,
-                   grid=self.grid, out=self.C, workspace=self.ws)
+                   grid=self.grid, out=self.C, workspace=self.ws, ntile=self.ntile)
 
     def run(self):
         """One launch over the whole batch (graph replay when captured)."""

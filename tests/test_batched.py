@@ -80,3 +80,23 @@ def test_batched_split_form_in_graph(cuda):
         ref = O.spmm_f64(m.rowptr, m.col, m.val, m.M, b)
         bound = O.spmm_absbound_f64(m.rowptr, m.col, m.val, m.M, b)
         assert (np.abs(c - ref) <= 2.0 ** -14 * bound + 1e-6).all()
+
+
+@pytest.mark.gpu
+def test_batched_autotune_then_graph(cuda):
+    """The autotuner's pick (window height, mode, CTA count, N-tiles) for the
+    batch keeps every matrix's product correct, also under graph replay."""
+    import torch
+    mats = _mats(16, seed=7)
+    N = 64
+    rng = np.random.default_rng(4)
+    bs = batched.BatchedSpMM(mats, N)
+    table = bs.autotune(reps=1)
+    assert set(table) == {16, 32} and bs.m.H in (16, 32)
+    bs.capture()
+    Bs = [rng.standard_normal((m.M, N)).astype(np.float32) for m in mats]
+    bs.load([torch.from_numpy(b).cuda() for b in Bs])
+    for m, b, c in zip(mats, Bs, [c.cpu().numpy() for c in bs.split(bs.run())]):
+        ref = O.spmm_f64(m.rowptr, m.col, m.val, m.M, b)
+        bound = O.spmm_absbound_f64(m.rowptr, m.col, m.val, m.M, b)
+        assert (np.abs(c - ref) <= TF32_TOL * bound + 1e-6).all()
