@@ -27,7 +27,10 @@
 // issuers 4-5, loaders 6-9 (cp.async of the planes), tile builders 10-13
 // (A_hi / A_lo tiles), converters 14-21 (wait for a stage's gathered rows,
 // rebuild the bf16 operand rows in place). A stage is released to the UMMA
-// issuers by one tile-builder and one converter arrival.
+// issuers by one tile-builder and one converter arrival. Finished C tiles
+// leave through shared memory and per-warp TMA tensor stores (16 rows x 32
+// columns). At window height 32 with one N-tile a stage holds 3 blocks, so
+// the 32-row A tiles and the staging fit in shared memory.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "spmm_sched.cuh"

@@ -21,7 +21,10 @@
 //
 // Pipeline. A ring of S stages, each holding P consecutive TC blocks of the
 // CTA's range (barrier traffic is per stage, not per block).
-//   warps 0-3   epilogue: tcgen05.ld 32x32b, coalesced stores of C rows
+//   warps 0-3   epilogue: tcgen05.ld 32x32b; each warp stages its 32 columns
+//               x window rows of C in shared memory and issues one TMA tensor
+//               store (plain per-lane stores stalled these warps and, through
+//               the accumulator hand-off, the whole pipeline)
 //   warps 4-5   UMMA issuers (one thread each; warp 4 also owns TMEM):
 //               issuer m takes the stages s % 2 == m into its own set of
 //               accumulators, so two MMA streams are in flight (a single
@@ -31,7 +34,8 @@
 //   warps 6-9   loaders: cp.async 16-byte gathers of B rows (SparseAToX),
 //               zero-fill for padded slots; stage s is owned by loader s % 4
 //   warps 10-13 tile builders: zero + scatter TC-block values into A_b^T;
-//               stage s is owned by tile builder s % 4
+//               stage s is owned by tile builder s % 4; tile ids and values
+//               of a stage are loaded one owned stage ahead
 // Each warp owns a fixed residue class of stages, so it waits on every
 // barrier phase of its stages in order (a parity wait more than one phase
 // ahead would pass spuriously). Every wait is bounded (2 s) and records
