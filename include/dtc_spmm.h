@@ -5,7 +5,10 @@
  * the current device, every call is asynchronous on `stream` unless stated,
  * and every call returns a dtc_status (never exits the process). The library
  * allocates no device memory: callers pass a workspace sized by the matching
- * *_workspace_bytes query.
+ * *_workspace_bytes query. The tcgen05 SpMM entry points read B and write C
+ * with 16-byte accesses and TMA stores: d_B / B planes and d_C must be 16-byte
+ * aligned and N a multiple of 4 (16 for the split-precision forms); other N
+ * go to the legacy-ISA kernel where an entry point says so.
  *
  * Each entry point names the reference interface it replaces (paths relative
  * to the reference project root, HPMLL/DTC-SpMM_ASPLOS24).
