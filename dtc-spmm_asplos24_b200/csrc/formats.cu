@@ -7,6 +7,9 @@
 //   BF16    : round-to-nearest-even bf16, 2 bytes/element.
 //   FP8     : e4m3 (satfinite, RNE) of B[r,:] / s_r with s_r = max|B[r,:]|/448,
 //             plus the fp32 per-row scale s_r. 1 byte/element + 4 bytes/row.
+//   BF16X2  : hi = bf16_rn(b), lo = bf16_rn(b - hi) (b - hi is exact in fp32;
+//             lo = 0 where hi is not finite), two bf16 planes: 4 bytes/element,
+//             hi + lo carries ~16 significant bits and needs no rebuild.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "common.cuh"
@@ -35,6 +38,18 @@ __global__ void k_pack_bf16(const float* __restrict__ B, int64_t n, __nv_bfloat1
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
     o[i] = __float2bfloat16_rn(B[i]);
+}
+
+__global__ void k_pack_bf16x2(const float* __restrict__ B, int64_t n, __nv_bfloat16* __restrict__ hi,
+                              __nv_bfloat16* __restrict__ lo) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float b = B[i];
+    const __nv_bfloat16 h = __float2bfloat16_rn(b);
+    const float hf = __bfloat162float(h);
+    hi[i] = h;
+    lo[i] = __float2bfloat16_rn(isfinite(hf) ? b - hf : 0.0f);
+  }
 }
 
 // One warp per row: scale = max|x| / 448, q = e4m3(x / scale).
@@ -74,6 +89,7 @@ dtc_status bformat_bytes_impl(int fmt, int64_t rows, int32_t N, size_t* b0, size
     case DTC_B_SPLIT24: *b0 = n * 2; *b1 = n; return DTC_OK;
     case DTC_B_BF16: *b0 = n * 2; *b1 = 0; return DTC_OK;
     case DTC_B_FP8: *b0 = n; *b1 = (size_t)rows * 4; return DTC_OK;
+    case DTC_B_BF16X2: *b0 = n * 2; *b1 = n * 2; return DTC_OK;
   }
   set_error("unknown B format");
   return DTC_ERR_INVALID_ARGUMENT;
@@ -95,6 +111,10 @@ dtc_status pack_b_impl(int fmt, const float* B, int64_t rows, int32_t N, void* p
       break;
     case DTC_B_BF16:
       k_pack_bf16<<<grid_for(n), 256, 0, st>>>(B, n, (__nv_bfloat16*)p0);
+      break;
+    case DTC_B_BF16X2:
+      DTC_REQUIRE(p1, "BF16X2 needs two planes");
+      k_pack_bf16x2<<<grid_for(n), 256, 0, st>>>(B, n, (__nv_bfloat16*)p0, (__nv_bfloat16*)p1);
       break;
     case DTC_B_FP8:
       DTC_REQUIRE(p1, "FP8 needs the scale plane");

@@ -9,6 +9,9 @@
 //   BF16    : bf16 plane (2 bytes/element); lo = 0.
 //   FP8     : e4m3 plane + fp32 row scale (1 byte/element); the tile warps
 //             expand q * scale[row] to bf16 hi; lo = 0.
+//   BF16X2  : bf16 hi plane + bf16 lo plane (4 bytes/element, the fp32 byte
+//             count): the loaders copy both planes straight into the operand
+//             tile, no rebuild on the CUDA cores.
 // A values are split the same way: A_hi = bf16(a), A_lo = bf16(a - A_hi).
 //
 // One UMMA per TC block and 128-feature tile computes every product term:
@@ -20,7 +23,7 @@
 //   D[:, r] + D[:, 16 + r] = (B_hi + B_lo) A_hi^T + (B_hi [+ B_lo]) A_lo^T.
 // The N = 32 instruction costs the same tensor-pipe time as N = 16, so the
 // full product takes one instruction per block, like the tf32 form, while
-// gathering 3 (SPLIT24), 2 (BF16) or 1 (FP8) bytes per element instead of 4.
+// gathering 3 (SPLIT24), 2 (BF16), 1 (FP8) or 4 (BF16X2) bytes per element.
 //
 // Schedule, work split and the deterministic reduction are the tf32
 // kernel's (spmm_tc.cu). Warp roles (704 threads): epilogue 0-3, UMMA
@@ -51,7 +54,7 @@ constexpr int kConvWarps = 8;
 constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 704
 constexpr int kTileBytes = 4096;  // per block and 128-feature tile: 16 K rows x 128 bf16
 
-enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2 };
+enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2, kFormBF16X2 = 3 };
 
 // WH = row-window height; the UMMA N dimension is 2 WH (A_hi^T | A_lo^T).
 template <int FORM, int NT, int P, int S, int WH>
@@ -66,7 +69,8 @@ struct SCfg {
   static constexpr int kYB = 64 * WH;  // 16 K x 2WH N bf16, K-major core matrices
   static constexpr int kStageX = P * NT * kTileBytes;
   static constexpr int kRowStage = NT * 128;  // staged bytes of one gathered row (u8 / e4m3)
-  static constexpr int kStageE = (FORM == kFormBF16) ? 0 : P * kBlkW * kRowStage;
+  static constexpr int kStageE =
+      (FORM == kFormBF16 || FORM == kFormBF16X2) ? 0 : P * kBlkW * kRowStage;
   static constexpr int kStageY = P * kYB;
   static constexpr int kX = S * kStageX;
   static constexpr int kE = S * kStageE;
@@ -136,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
     *abort_flag = 0;
     fence_mbar_init();
   }
-  if (FORM != kFormSplit24) {  // lo rows stay zero for the single-plane forms
+  if (FORM == kFormBF16 || FORM == kFormFP8) {  // lo rows stay zero for one-plane forms
     for (int i = threadIdx.x; i < S * P * NT; i += blockDim.x) {
       float4* lo = reinterpret_cast<float4*>(xring + (size_t)i * kTileBytes + 2048);
       for (int z = 0; z < 2048 / 16; ++z) lo[z] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -184,24 +188,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
         // full 128-feature tiles: RPI gathered rows per warp instruction,
         // CPR 16-byte chunks per row (compile-time)
         for (int pb = 0; pb < nb; ++pb) {
-          if (FORM != kFormFP8) {  // bf16 hi plane -> K row k of the block tile, swizzled
+          if (FORM != kFormFP8) {  // bf16 hi (+ lo) plane -> K rows of the block tile, swizzled
             constexpr int CPR = NT * 16, RPI = CPR >= 32 ? 1 : 32 / CPR;
             constexpr int IPR = CPR >= 32 ? CPR / 32 : 1;
+            constexpr int NPL = FORM == kFormBF16X2 ? 2 : 1;  // plane pl -> K rows 8 pl .. 8 pl + 7
 #pragma unroll
-            for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
-              const int k = k0 + (RPI > 1 ? lane / CPR : 0);
-              const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
-              const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
-              const uint8_t* src = plane0 + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
+            for (int pl = 0; pl < NPL; ++pl) {
+              const uint8_t* base = pl ? plane1 : plane0;
 #pragma unroll
-              for (int ii = 0; ii < IPR; ++ii) {
-                const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
-                cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(k, cc & 15),
-                           src + cc * 16, pad ? 0u : 16u);
+              for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
+                const int k = k0 + (RPI > 1 ? lane / CPR : 0);
+                const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+                const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
+                const uint8_t* src = base + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
+#pragma unroll
+                for (int ii = 0; ii < IPR; ++ii) {
+                  const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
+                  cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes +
+                                 x_offset_bf16(pl * 8 + k, cc & 15),
+                             src + cc * 16, pad ? 0u : 16u);
+                }
               }
             }
           }
-          if (FORM != kFormBF16) {  // u8 extension / e4m3 plane -> staging row
+          if (FORM == kFormSplit24 || FORM == kFormFP8) {  // u8 ext / e4m3 plane -> staging
             constexpr int CPR = NT * 8, RPI = CPR >= 32 ? 1 : 32 / CPR;
             constexpr int IPR = CPR >= 32 ? CPR / 32 : 1;
 #pragma unroll
@@ -226,17 +236,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
         const int nrow = nb * kBlkW;
         if (FORM != kFormFP8) {
           const int nck = ncols >> 3;
-          for (int idx = lane; idx < nrow * nck; idx += 32) {
-            const int rowi = idx / nck, cc = idx - rowi * nck;
+          constexpr int NPL = FORM == kFormBF16X2 ? 2 : 1;
+          for (int idx = lane; idx < NPL * nrow * nck; idx += 32) {
+            const int pl = idx / (nrow * nck), id2 = idx - pl * nrow * nck;
+            const int rowi = id2 / nck, cc = id2 - rowi * nck;
             const int k = rowi & 7, pb = rowi >> 3;
             const int32_t r = rows_sm[lw][rowi];
             const bool pad = (k > 0 && r == 0);
-            const uint8_t* src = plane0 + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
-            cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(k, cc & 15),
+            const uint8_t* src = (pl ? plane1 : plane0) + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
+            cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(pl * 8 + k, cc & 15),
                        src + cc * 16, pad ? 0u : 16u);
           }
         }
-        if (FORM != kFormBF16) {
+        if (FORM == kFormSplit24 || FORM == kFormFP8) {
           const int nck = ncols >> 4;
           for (int idx = lane; idx < nrow * nck; idx += 32) {
             const int rowi = idx / nck, cc = idx - rowi * nck;
@@ -348,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
         row_scale[cw][lane] = scv;
         __syncwarp();
       }
-      if (FORM != kFormBF16) {
+      if (FORM == kFormSplit24 || FORM == kFormFP8) {
         uint8_t* xs = xring + (size_t)s * K::kStageX;
         const uint8_t* es = ering + (size_t)s * K::kStageE;
         const int items = nb * kBlkW * nchunk;
@@ -647,8 +659,9 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            int precision, float* C, int mode, int grid, float* part,
                            cudaStream_t st, int ntile, Epilogue epi, int H) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
-  DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8,
-              "split kernels take SPLIT24, BF16 or FP8 B");
+  DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8 ||
+                  bformat == DTC_B_BF16X2,
+              "split kernels take SPLIT24, BF16, FP8 or BF16X2 B");
   DTC_REQUIRE(precision == DTC_PREC_SPLIT3 || precision == DTC_PREC_SPLIT4,
               "split kernels take precision SPLIT3 or SPLIT4");
   DTC_REQUIRE(N % 16 == 0, "split forms need N % 16 == 0 (16-byte row segments of every plane)");
@@ -686,6 +699,9 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
     case DTC_B_BF16:
       return four ? dispatch_n<kFormBF16, true>(p, st, ntile)
                   : dispatch_n<kFormBF16, false>(p, st, ntile);
+    case DTC_B_BF16X2:
+      return four ? dispatch_n<kFormBF16X2, true>(p, st, ntile)
+                  : dispatch_n<kFormBF16X2, false>(p, st, ntile);
     default:
       return four ? dispatch_n<kFormFP8, true>(p, st, ntile)
                   : dispatch_n<kFormFP8, false>(p, st, ntile);

@@ -6,5 +6,6 @@ this package is the Python front end over the same C ABI (libdtcspmm.so):
 inputs).
 """
 from . import _lib  # noqa: F401
-from ._lib import (B_BF16, B_F32, B_FP8, B_SPLIT24, PREC_SPLIT3, PREC_SPLIT4,  # noqa: F401
+from ._lib import (B_BF16, B_BF16X2, B_F32, B_FP8, B_SPLIT24,  # noqa: F401
+                   PREC_SPLIT3, PREC_SPLIT4,
                    PREC_TF32, DtcError)

@@ -94,7 +94,7 @@ class Schedule(C.Structure):
         return (f"Schedule(mode={self.mode}, waves={self.waves}, ntile={self.ntile}, "
                 f"grid={self.grid}, ms={self.ms:.4f})")
 
-B_F32, B_SPLIT24, B_BF16, B_FP8 = 0, 1, 2, 3
+B_F32, B_SPLIT24, B_BF16, B_FP8, B_BF16X2 = 0, 1, 2, 3, 4
 PREC_TF32, PREC_SPLIT3, PREC_SPLIT4 = 0, 1, 2
 
 

@@ -9,8 +9,9 @@ The reference fixes its schedule by hand per dataset and N
 with row windows of 16 or 32 rows and TC blocks 8 columns wide (the kernels'
 compaction width), mode 0 (window-scheduled) or 1 (strict
 balance; the split threshold is ceil(T / CTAs) blocks), waves in {1,2,4,8,16}
-(CTAs = waves x SMs), N-tiles per CTA in {1,2,4}, the two B forms within
-1e-5 relative error (SPLIT24 with 4- or 3-term products) and TCA reorder off or
+(CTAs = waves x SMs), N-tiles per CTA in {1,2,4}, two B forms within 1e-5
+relative error (SPLIT24, 3 bytes per element rebuilt on chip, and BF16X2, 4
+bytes per element used as stored; both with 3-term products) and TCA reorder off or
 on. The network predicts, for every class, log(t_class / t_best) of the SpMM
 kernel; it is trained on timings the library measures itself on seeded
 synthetic matrices (``collect``), entirely with the library's own CUDA kernels
@@ -36,7 +37,7 @@ NFEAT = 48
 HEIGHTS = (16, 32)
 WAVES = (1, 2, 4, 8, 16)
 NTILES = (1, 2, 4)
-FORMS = ("split24x4", "split24x3")
+FORMS = ("split24x3", "bf16x2x3")
 CLASSES = [dict(H=h, W=8, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
            for ro in (0, 1) for h in HEIGHTS for fo in FORMS for mo in (0, 1) for wv in WAVES
            for nt in NTILES]
@@ -67,8 +68,8 @@ def class_of(mode, waves, ntile, form, reorder, H=16):
 
 def default_class(N):
     """The untuned library default for width N (window height 16, strict
-    balance, 16 waves, all N-tiles in one CTA, SPLIT24 4-term, no reorder)."""
-    return class_of(1, 16, auto_ntile(N), "split24x4", 0, 16)
+    balance, 16 waves, all N-tiles in one CTA, SPLIT24 3-term, no reorder)."""
+    return class_of(1, 16, auto_ntile(N), "split24x3", 0, 16)
 
 
 # ----------------------------------------------------------------- features

@@ -14,8 +14,8 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib
-from ._lib import (B_BF16, B_F32, B_FP8, B_SPLIT24, PREC_SPLIT3, PREC_SPLIT4, PREC_TF32,
-                   Schedule, call)
+from ._lib import (B_BF16, B_BF16X2, B_F32, B_FP8, B_SPLIT24, PREC_SPLIT3, PREC_SPLIT4,
+                   PREC_TF32, Schedule, call)
 from .metcf import METCF, _ptr, _stream, pack_b, spmm_ex
 
 # name -> (B storage form, product precision, B bytes per element, relative
@@ -26,6 +26,7 @@ FORMS = {
     "tf32": (B_F32, PREC_TF32, 4.0, 1e-3),
     "split24x4": (B_SPLIT24, PREC_SPLIT4, 3.0, 1e-5),
     "split24x3": (B_SPLIT24, PREC_SPLIT3, 3.0, 1e-5),
+    "bf16x2x3": (B_BF16X2, PREC_SPLIT3, 4.0, 1e-5),
     "bf16": (B_BF16, PREC_SPLIT4, 2.0, 1e-2),
     "fp8": (B_FP8, PREC_SPLIT4, 1.0, 1e-1),
 }

@@ -154,7 +154,9 @@ typedef enum {
   DTC_B_SPLIT24 = 1,  /* bf16 hi plane [rows*N] + u8 extension plane [rows*N]: */
                       /* fp32 rounded to 16 significant bits, 3 bytes/element  */
   DTC_B_BF16 = 2,     /* bf16 rows                                              */
-  DTC_B_FP8 = 3       /* e4m3 plane [rows*N] + fp32 per-row scale [rows]        */
+  DTC_B_FP8 = 3,      /* e4m3 plane [rows*N] + fp32 per-row scale [rows]        */
+  DTC_B_BF16X2 = 4    /* bf16 hi plane + bf16 lo plane, lo = bf16(b - hi):      */
+                      /* 4 bytes/element, ~16 significant bits, no rebuild      */
 } dtc_bformat;
 
 typedef enum {

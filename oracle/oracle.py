@@ -146,6 +146,23 @@ def pack_bf16(B):
     return out
 
 
+def pack_bf16x2(B):
+    """BF16X2 planes: hi = bf16_rn(b), lo = bf16_rn(b - hi) (the difference is
+    exact in fp32), lo = 0 where hi is not finite. Returns (hi, lo) uint16."""
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    hi = pack_bf16(B)
+    hf = (hi.astype(np.uint32) << 16).view(np.float32)
+    with np.errstate(invalid="ignore", over="ignore"):
+        d = np.where(np.isfinite(hf), B - hf, np.float32(0)).astype(np.float32)
+    return hi, pack_bf16(d)
+
+
+def bf16x2_values(hi, lo):
+    """hi + lo as float64 (the value the BF16X2 planes stand for)."""
+    f = lambda u: (u.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+    return f(hi) + f(lo)
+
+
 def pack_fp8(B):
     """fp32 rows -> (e4m3 bytes, fp32 per-row scales)."""
     B = np.ascontiguousarray(B, dtype=np.float32)

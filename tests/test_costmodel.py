@@ -49,7 +49,7 @@ def test_class_space():
     assert cm.feasible(512).sum() == cm.K // 2 + cm.K // 3
     d = cm.CLASSES[cm.default_class(512)]
     assert (d["H"], d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == \
-        (16, 1, 16, 4, "split24x4", 0)
+        (16, 1, 16, 4, "split24x3", 0)
     assert {c["H"] for c in cm.CLASSES} == {16, 32} and all(c["W"] == 8 for c in cm.CLASSES)
     assert len({cm.class_of(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"])
                 for c in cm.CLASSES}) == cm.K

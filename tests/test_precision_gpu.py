@@ -67,8 +67,23 @@ def test_pack_fp8_bit_exact(cuda):
     np.testing.assert_array_equal(_u8(p0).reshape(B.shape), q)
 
 
+def test_pack_bf16x2_bit_exact(cuda):
+    import torch
+    from dtc_b200 import metcf, B_BF16X2
+    B = _special_B(seed=3)
+    hi, lo = O.pack_bf16x2(B)
+    p0, p1 = metcf.pack_b(torch.from_numpy(B).cuda(), B_BF16X2)
+    gh = _u8(p0).view(np.uint16).reshape(B.shape)
+    gl = _u8(p1).view(np.uint16).reshape(B.shape)
+    ok = ~np.isnan(B)
+    np.testing.assert_array_equal(gh[ok], hi[ok])
+    np.testing.assert_array_equal(gl[ok], lo[ok])
+
+
 def _stored_B(fmt, B):
-    from dtc_b200 import B_BF16, B_FP8, B_SPLIT24
+    from dtc_b200 import B_BF16, B_BF16X2, B_FP8, B_SPLIT24
+    if fmt == B_BF16X2:
+        return O.bf16x2_values(*O.pack_bf16x2(B)).astype(np.float32)
     if fmt == B_SPLIT24:
         return O.split24_values(*O.pack_split24(B))
     if fmt == B_BF16:
@@ -114,6 +129,17 @@ def test_split24_forms(cuda, name, N, prec, mode):
     from dtc_b200 import B_SPLIT24
     rp, col, val, M, B, C = _run_form(name, N, B_SPLIT24, prec, mode)
     _assert_close(C, rp, col, val, M, _stored_B(B_SPLIT24, B), 2.0 ** -15, "stored B")
+    _assert_close(C, rp, col, val, M, B, 2.0 ** -14, "original B")
+
+
+@pytest.mark.parametrize("name", ["small_uniform", "hub", "banded_dense", "empty_windows"])
+@pytest.mark.parametrize("N", [16, 128, 272])
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_bf16x2_forms(cuda, name, N, prec, mode):
+    from dtc_b200 import B_BF16X2
+    rp, col, val, M, B, C = _run_form(name, N, B_BF16X2, prec, mode)
+    _assert_close(C, rp, col, val, M, _stored_B(B_BF16X2, B), 2.0 ** -15, "stored B")
     _assert_close(C, rp, col, val, M, B, 2.0 ** -14, "original B")
 
 

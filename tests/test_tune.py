@@ -22,7 +22,7 @@ def test_candidates_cover_modes_waves_ntiles():
 
 
 def test_forms_by_error_budget():
-    assert set(tune.eligible_forms(1e-5)) == {"split24x4", "split24x3"}
+    assert set(tune.eligible_forms(1e-5)) == {"split24x4", "split24x3", "bf16x2x3"}
     assert "tf32" in tune.eligible_forms(1e-3)
     assert tune.eligible_forms(1e-9) == []
 
@@ -68,6 +68,6 @@ def test_tune_forms_picks_within_budget(cuda):
     m = metcf.convert(A.rowptr, A.col, A.M, values=A.val)
     B = torch.from_numpy(gen.normal(A.M, 128, seed=2)).cuda()
     best, table = tune.tune_forms(m, B, max_rel_err=1e-5, reps=1)
-    assert set(table) == {"split24x4", "split24x3"}
+    assert set(table) == {"split24x4", "split24x3", "bf16x2x3"}
     assert best.form in table
     assert best.ms == min(s.ms for v in table.values() for s in v)

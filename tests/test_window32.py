@@ -36,7 +36,7 @@ def test_convert_h32_bit_exact(cuda, name):
 @pytest.mark.parametrize("name", ["small_uniform", "hub", "empty_windows", "banded_dense"])
 @pytest.mark.parametrize("form,N", [("tf32", 36), ("tf32", 128), ("tf32", 520),
                                     ("split24x4", 16), ("split24x4", 272), ("split24x3", 128),
-                                    ("bf16", 64), ("fp8", 32)])
+                                    ("bf16x2x3", 128), ("bf16", 64), ("fp8", 32)])
 @pytest.mark.parametrize("mode", [0, 1])
 def test_spmm_h32(cuda, name, form, N, mode):
     import torch
@@ -51,7 +51,7 @@ def test_spmm_h32(cuda, name, form, N, mode):
         C = metcf.spmm_ex(m, planes, fmt, N, prec, mode=mode, grid=grid).cpu().numpy()
         if form == "tf32":
             _bound_ok(C, rp, col, val, M, B, 2.0 ** -9)
-        elif form.startswith("split24"):
+        elif form.startswith("split24") or form == "bf16x2x3":
             _bound_ok(C, rp, col, val, M, B, 2.0 ** -14)
         elif form == "bf16":
             _bound_ok(C, rp, col, val, M, B, 2.0 ** -8)
