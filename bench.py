@@ -304,7 +304,8 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from dtc_b200 import metcf, replicas, B_F32, B_SPLIT24, B_BF16, B_FP8, PREC_TF32, PREC_SPLIT3, PREC_SPLIT4
+    from dtc_b200 import (metcf, replicas, B_F32, B_SPLIT24, B_BF16, B_FP8, B_BF16X2, PREC_TF32,
+                          PREC_SPLIT3, PREC_SPLIT4)
     import DTCSpMM
 
     A, Bh, N, name = make_workload(args)
@@ -315,6 +316,7 @@ def main():
     peaks, peak_kind = load_peaks()
 
     planes = {B_SPLIT24: metcf.pack_b(B, B_SPLIT24), B_BF16: metcf.pack_b(B, B_BF16),
+              B_BF16X2: metcf.pack_b(B, B_BF16X2),
               B_FP8: metcf.pack_b(B, B_FP8)}
     outs = {}
 
@@ -338,6 +340,7 @@ def main():
         "split24x4_window": (ex(B_SPLIT24, PREC_SPLIT4, 0, "split24x4_window"), 3.0, 1),
         "split24x4_balance": (ex(B_SPLIT24, PREC_SPLIT4, 1, "split24x4_balance"), 3.0, 2),
         "split24x3_balance": (ex(B_SPLIT24, PREC_SPLIT3, 1, "split24x3_balance"), 3.0, 2),
+        "bf16x2x3_balance": (ex(B_BF16X2, PREC_SPLIT3, 1, "bf16x2x3_balance"), 4.0, 2),
         "bf16_balance": (ex(B_BF16, PREC_SPLIT4, 1, "bf16_balance"), 2.0, 2),
         "fp8_balance": (ex(B_FP8, PREC_SPLIT4, 1, "fp8_balance"), 1.0 + 4.0 / N, 2),
     }
@@ -379,7 +382,7 @@ def main():
     tuned_tbl = {}
     for H, mm in mets.items():
         ws_t = tune.workspace_for(mm, N, dev)
-        for fo in ("tf32", "split24x4", "split24x3"):
+        for fo in ("tf32", "split24x4", "split24x3", "bf16x2x3"):
             fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
             pl = [B] if fo == "tf32" else planes[fmt]
             scheds, best = tune.autotune(mm, pl, fmt, N, prec, reps=3, out=out_for("tune"),
@@ -479,7 +482,8 @@ def main():
     cpu, errs = (None, {})
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu, _ = cpu_baseline(A, Bh, N)
-        for k in (tf32_best, "split24x3_balance", "bf16_balance", "fp8_balance"):
+        for k in (tf32_best, "split24x3_balance", "bf16x2x3_balance", "bf16_balance",
+                  "fp8_balance"):
             forms[k][0]()
             torch.cuda.synchronize()
             errs[k] = accuracy_vs_fp64(A, Bh, N, outs[k].cpu().numpy())
