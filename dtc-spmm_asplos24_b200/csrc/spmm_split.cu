@@ -32,8 +32,9 @@
 // rebuild the bf16 operand rows in place). A stage is released to the UMMA
 // issuers by one tile-builder and one converter arrival. Finished C tiles
 // leave through shared memory and per-warp TMA tensor stores (16 rows x 32
-// columns). At window height 32 with one N-tile a stage holds 3 blocks, so
-// the 32-row A tiles and the staging fit in shared memory.
+// columns). At window height 32 with one N-tile, the forms that stage a
+// second plane (SPLIT24, FP8) hold 3 blocks per stage so the 32-row A tiles
+// and the staging fit in shared memory.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "spmm_sched.cuh"
@@ -642,8 +643,11 @@ template <int FORM, bool FOUR>
 dtc_status dispatch_n(const Params& p, cudaStream_t st, int ntile) {
   int nt = p.N <= 128 ? 1 : p.N <= 256 ? 2 : 4;
   if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
-  if (p.H == 32) {  // 3 blocks per stage keep the 32-row A tiles within shared memory
-    if (nt == 1) return launch_split<FORM, 1, 3, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
+  if (p.H == 32) {
+    // forms with a staging ring for the second plane hold 3 blocks per stage so
+    // the 32-row A tiles fit in shared memory; the others keep 4
+    constexpr int P32 = (FORM == kFormBF16 || FORM == kFormBF16X2) ? 4 : 3;
+    if (nt == 1) return launch_split<FORM, 1, P32, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
     return launch_split<FORM, 2, 2, 8, FOUR, 32>(p, (p.N + 255) / 256, st);
   }
   if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 16>(p, (p.N + 127) / 128, st);
