@@ -196,3 +196,24 @@ def test_scheduler_verifies_top_predictions(cuda):
     ok = np.flatnonzero(cm.feasible(128))
     top = set(ok[np.argsort(y[ok], kind="stable")[:3]].tolist())
     assert plain.cls in top and ver.cls in top
+
+
+def test_committed_weights_beat_default_on_held_out_cpu():
+    """The shipped network, evaluated by the FP64 oracle forward pass on the
+    committed held-out matrices (no GPU): its choices beat the untuned default
+    and stay close to the exhaustive best."""
+    if not (os.path.exists(cm.DATASET_PATH) and os.path.exists(cm.WEIGHTS_PATH)):
+        pytest.skip("no dataset / weights committed")
+    z = np.load(cm.WEIGHTS_PATH)
+    dims = tuple(int(d) for d in z["dims"])
+    assert dims == DIMS
+    ds = cm.load_dataset()
+    tr, N = cm.split(ds)
+    _, _, Y = CO.forward(z["params"], dims, ds["features"][~tr])
+    choices = []
+    for y, n in zip(Y, N[~tr]):
+        ok = np.flatnonzero(cm.feasible(int(n)))
+        choices.append(int(ok[np.argmin(y[ok])]))
+    ev = cm.evaluate(np.array(choices), ds["times"][~tr], N[~tr], pred=Y)
+    assert ev["speedup_vs_default_geomean"] > 1.5, ev
+    assert ev["regret_mean"] < 0.05 and ev["regret_top4_mean"] < 0.01, ev
