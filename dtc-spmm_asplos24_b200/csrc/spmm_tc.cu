@@ -421,13 +421,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const __grid_constant
   }
 }
 
+// rwo[w] = first block of window w, from the sorted window id of every block.
+// Ids come from the caller: an id outside [0, nwin) or a descending pair is
+// reported through kErrBadIndex, and the written range is clamped to the
+// (nwin + 1)-entry table, so a bad id never writes outside it.
 __global__ void k_rowid_to_rwo(const int32_t* __restrict__ rowid, int64_t T, int32_t nwin,
-                               int32_t* __restrict__ rwo) {
+                               int32_t* __restrict__ rwo, uint32_t* err) {
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b <= T; b += stride) {
     const int32_t prev = (b == 0) ? -1 : __ldg(rowid + b - 1);
     const int32_t cur = (b == T) ? nwin : __ldg(rowid + b);
-    for (int32_t w = prev + 1; w <= cur; ++w) rwo[w] = (int32_t)b;
+    const bool bad = (b < T && (cur < 0 || cur >= nwin)) || cur < prev;
+    if (bad) atomicOr(err, kErrBadIndex);
+    const int32_t lo = prev < -1 ? -1 : (prev > nwin ? nwin : prev);
+    const int32_t hi = cur < -1 ? -1 : (cur > nwin ? nwin : cur);
+    for (int32_t w = lo + 1; w <= hi; ++w) rwo[w] = (int32_t)b;
   }
 }
 
@@ -510,7 +518,7 @@ dtc_status rowid_to_rwo(const int32_t* rowid, int64_t T, int32_t nwin, int32_t* 
   int64_t n = T + 1;
   unsigned g = (unsigned)((n + 255) / 256);
   if (g > 65535u * 16) g = 65535u * 16;
-  k_rowid_to_rwo<<<g, 256, 0, st>>>(rowid, T, nwin, rwo);
+  k_rowid_to_rwo<<<g, 256, 0, st>>>(rowid, T, nwin, rwo, device_error_word());
   DTC_CUDA(cudaGetLastError());
   return DTC_OK;
 }

@@ -148,6 +148,23 @@ def pack_b_into(B: torch.Tensor, fmt: int, planes):
     return planes
 
 
+def spmm_ex_workspace_bytes(m: METCF, N, mode=0, grid=0):
+    """Workspace bytes spmm_ex needs for this schedule (0 in window mode)."""
+    wsb = C.c_size_t()
+    call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, m.H, mode, grid, C.byref(wsb))
+    return wsb.value
+
+
+def spmm_ex_launches(m: METCF, mode=0, grid=0):
+    """Kernels one spmm_ex call launches: the SpMM, plus the partial-tile
+    reduction in balance mode when more than one CTA shares the blocks."""
+    if m.T == 0:
+        return 0
+    sms = torch.cuda.get_device_properties(m.RowWindowOffset.device).multi_processor_count
+    G = min(grid if grid > 0 else 16 * sms, m.T)
+    return 2 if (mode == 1 and G > 1) else 1
+
+
 def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True, out=None,
             workspace=None, ntile=0):
     if m.W != 8:

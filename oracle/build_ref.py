@@ -1,7 +1,9 @@
 """Build recipe for the UNMODIFIED reference extension (test infrastructure).
 
-Compiles the reference's two translation units, where they lie under
-/root/reference/DTC-SpMM, into ``oracle/_ref/DTCSpMM*.so`` for sm_100a. Nothing is
+Compiles the reference's two translation units, where they lie in the
+reference checkout (its DTC-SpMM/ folder; the checkout's root is taken from the
+DTC_REFERENCE_ROOT environment variable, default /root/reference), into
+``oracle/_ref/DTCSpMM*.so`` for sm_100a. Nothing is
 copied out of the reference tree; the only addition is the sputnik stub header
 under ``oracle/sputnik_stub`` (sputnik is an un-vendored submodule of the
 reference; only its competitor-baseline entry point needs it).
@@ -11,8 +13,8 @@ The product never loads this library. It is used only
 * by ``tests/golden/make_golden.py`` to produce golden ME-TCF vectors from the
   reference's own ``preprocess`` (CPU) and ``preprocess_gpu`` (GPU) entry points,
 * by ``-m gpu`` tests, when present, as a second bit-exactness check,
-* by ``bench.py --impl reference-sm100a`` to time the reference's kernels
-  rebuilt for sm_100a.
+* by ``bench.py --impl reference`` to time the reference's own conversion and
+  kernels rebuilt for sm_100a.
 
 Usage: ``python oracle/build_ref.py`` (no-op when the reference tree is absent,
 e.g. on a GPU box that received the prebuilt ``oracle/_ref``).
@@ -23,7 +25,8 @@ import sys
 import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/DTC-SpMM"
+REF_ROOT = os.environ.get("DTC_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "DTC-SpMM")
 OUT = os.path.join(HERE, "_ref")
 EXT_SUFFIX = sysconfig.get_config_var("EXT_SUFFIX")
 TARGET = os.path.join(OUT, "DTCSpMM" + EXT_SUFFIX)

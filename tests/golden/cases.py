@@ -90,6 +90,30 @@ def hub(seed=5):
     return rp, c, _vals(len(c), seed + 100), M
 
 
+def rmat12(seed=7):
+    """R-MAT (0.57, 0.19, 0.19, 0.05), 2^12 nodes, 16 * 2^12 generated edges,
+    symmetrised, self-loops added, duplicates removed (numpy-generated): the
+    power-law shape of the benchmark at a size the golden files can carry."""
+    rng = np.random.default_rng(seed)
+    scale, M = 12, 1 << 12
+    ne = 16 * M
+    probs = np.array([0.57, 0.19, 0.19, 0.05])
+    src = np.zeros(ne, np.int64)
+    dst = np.zeros(ne, np.int64)
+    for _ in range(scale):
+        q = rng.choice(4, size=ne, p=probs)
+        src = 2 * src + (q >> 1)
+        dst = 2 * dst + (q & 1)
+    r = np.concatenate([src, dst, np.arange(M)])
+    c = np.concatenate([dst, src, np.arange(M)])
+    key = np.unique(r * M + c)
+    r, c = key // M, key % M
+    rowptr = np.zeros(M + 1, np.int32)
+    rowptr[1:] = np.cumsum(np.bincount(r, minlength=M))
+    col = c.astype(np.int32)
+    return rowptr, col, _vals(len(col), seed + 100), M
+
+
 def banded_dense(seed=6):
     """Dense band: full 16 x 8 TC blocks (128 nonzeros per block)."""
     M = 256
@@ -106,9 +130,29 @@ CASES = {
     "wide_window": wide_window,
     "hub": hub,
     "banded_dense": banded_dense,
+    "rmat12": rmat12,
 }
 
 # cases the reference's CPU `preprocess` handles safely (it has no empty-window
 # guard: DTC-SpMM/DTCSpMM.cpp:281-297)
 CPU_REFERENCE_SAFE = ["small_uniform", "uniform_4096", "duplicates", "wide_window", "hub",
-                      "banded_dense"]
+                      "banded_dense", "rmat12"]
+
+# (block_h, block_w) shapes the reference's preprocess_gpu was run with. The
+# 16 x 8 files keep their original names (ref_gpu_<case>.npz); the others carry
+# the shape: ref_gpu_h<H>w<W>__<case>.npz.
+GOLDEN_SHAPES = [(16, 8), (32, 8), (16, 16)]
+
+
+def golden_name(case, H=16, W=8):
+    return f"ref_gpu_{case}.npz" if (H, W) == (16, 8) else f"ref_gpu_h{H}w{W}__{case}.npz"
+
+
+def parse_golden_name(fname):
+    """ref_gpu_[h<H>w<W>__]<case>.npz -> (case, H, W)."""
+    stem = fname[len("ref_gpu_"):-len(".npz")]
+    if "__" in stem:
+        shape, case = stem.split("__", 1)
+        H, W = shape[1:].split("w")
+        return case, int(H), int(W)
+    return stem, 16, 8

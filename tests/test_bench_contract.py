@@ -1,5 +1,7 @@
-"""bench.py's reference (host CPU) arm prints one JSON line with the keys the
-benchmark contract needs; runs without a GPU on the small uniform config."""
+"""bench.py's reference arm prints one JSON line with the keys the benchmark
+contract needs and the same metric string as this library's arm. Without a
+GPU (here) the arm falls back to the host CSR SpMM port; runs on the small
+uniform config."""
 import json
 import os
 import subprocess
@@ -21,5 +23,8 @@ def test_reference_arm_json_line():
               "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["metric"] == bench.METRIC
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0

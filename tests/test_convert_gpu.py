@@ -41,14 +41,16 @@ def test_convert_bit_exact_vs_oracle(cuda, name):
 
 
 @pytest.mark.parametrize("name", list(cases.CASES))
-def test_convert_bit_exact_vs_reference_golden(cuda, name):
-    path = os.path.join(GOLDEN, f"ref_gpu_{name}.npz")
+@pytest.mark.parametrize("hw", cases.GOLDEN_SHAPES, ids=lambda hw: f"{hw[0]}x{hw[1]}")
+def test_convert_bit_exact_vs_reference_golden(cuda, name, hw):
+    H, W = hw
+    path = os.path.join(GOLDEN, cases.golden_name(name, H, W))
     if not os.path.exists(path):
         pytest.skip("reference golden vector not generated")
     g = dict(np.load(path))
     g["T"] = int(g["T"])
     rp, col, _, M = cases.CASES[name]()
-    _assert_same(_gpu_convert(rp, col, M), g, name)
+    _assert_same(_gpu_convert(rp, col, M, H=H, W=W), g, f"{name} {H}x{W}")
 
 
 @pytest.mark.parametrize("hw", [(16, 8), (16, 16), (32, 8), (8, 8)])
@@ -68,6 +70,30 @@ def test_convert_generated_configs(cuda):
         exp = O.metcf(m.rowptr, m.col, m.M, values=m.val)
         _assert_same(got, exp, "generated")
         np.testing.assert_array_equal(got["TCvalues"], exp["TCvalues"])
+
+
+def _full_size(name):
+    from dtc_b200 import gen
+    if name == "uniform_4096":
+        return gen.uniform(4096, mean=8.0, seed=0)
+    if name == "rmat20":
+        return gen.rmat(20, 16.0, 0.57, 0.19, 0.19, seed=0)
+    return gen.stencil27(126, seed=0)
+
+
+@pytest.mark.parametrize("name,H,W", [("uniform_4096", 16, 8), ("rmat20", 16, 8),
+                                      ("rmat20", 32, 8), ("rmat20", 16, 16),
+                                      ("stencil126", 16, 8), ("stencil126", 32, 8)])
+def test_convert_full_size_configs(cuda, name, H, W):
+    """Every ME-TCF array at the benchmark sizes, bit-exact with the oracle:
+    uniform 4096^2 Poisson(8), R-MAT 2^20 symmetrised + I (32.5 M nnz, hub
+    windows of ~15k TC blocks) and the 27-point stencil on 126^3 (2,000,376
+    rows, num_nodes % 16 == 8)."""
+    A = _full_size(name)
+    got = _gpu_convert(A.rowptr, A.col, A.M, A.val, H=H, W=W)
+    exp = O.metcf(A.rowptr, A.col, A.M, H=H, W=W, values=A.val)
+    _assert_same(got, exp, f"{name} {H}x{W}")
+    np.testing.assert_array_equal(got["TCvalues"], exp["TCvalues"])
 
 
 def test_convert_empty_matrix(cuda):

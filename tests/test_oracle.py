@@ -33,24 +33,27 @@ def _gpu_golden():
     return sorted(glob.glob(os.path.join(GOLDEN, "ref_gpu_*.npz")))
 
 
-@pytest.mark.parametrize("path", _gpu_golden() or [None])
+@pytest.mark.parametrize("path", _gpu_golden() or [None],
+                         ids=lambda p: os.path.basename(p) if p else "none")
 def test_oracle_matches_reference_gpu_preprocess(path):
+    """Every block shape the reference was run with (16 x 8, 32 x 8, 16 x 16)."""
     if path is None:
         pytest.skip("no reference preprocess_gpu golden vectors present")
-    name = os.path.basename(path)[len("ref_gpu_"):-len(".npz")]
+    name, H, W = cases.parse_golden_name(os.path.basename(path))
     g = np.load(path)
     rp, col, _, M = cases.CASES[name]()
-    m = O.metcf(rp, col, M)
+    m = O.metcf(rp, col, M, H=H, W=W)
     assert m["T"] == int(g["T"])
     for k in ARRAYS:
-        np.testing.assert_array_equal(m[k], g[k], err_msg=f"{name}:{k}")
+        np.testing.assert_array_equal(m[k], g[k], err_msg=f"{name} {H}x{W}:{k}")
 
 
-def test_gpu_golden_present_for_every_case():
-    names = {os.path.basename(p)[8:-4] for p in _gpu_golden()}
-    if not names:
+def test_gpu_golden_present_for_every_case_and_shape():
+    found = {cases.parse_golden_name(os.path.basename(p)) for p in _gpu_golden()}
+    if not found:
         pytest.skip("reference GPU golden vectors not generated yet")
-    assert names == set(cases.CASES)
+    want = {(n, H, W) for n in cases.CASES for H, W in cases.GOLDEN_SHAPES}
+    assert found == want, sorted(want - found)
 
 
 @pytest.mark.parametrize("name", list(cases.CASES))
@@ -92,3 +95,31 @@ def test_fp32_baseline_close_to_fp64():
     B = np.random.default_rng(3).standard_normal((M, 32)).astype(np.float32)
     np.testing.assert_allclose(O.spmm_f32(rp, col, val, M, B, nthreads=2),
                                O.spmm_f64(rp, col, val, M, B), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("path", [p for p in _gpu_golden()
+                                  if cases.parse_golden_name(os.path.basename(p))[1:] == (16, 8)]
+                         or [None], ids=lambda p: os.path.basename(p) if p else "none")
+def test_reference_spmm_golden_within_tf32_of_fp64(path):
+    """The reference's own SpMM outputs (A = 1) are TF32 products of the FP64
+    oracle's: N = 32 (float_nonsplit) and N = 128 (float4_split, stored rows)."""
+    if path is None:
+        pytest.skip("no reference golden vectors")
+    from tests.golden import make_golden
+    g = np.load(path)
+    name = cases.parse_golden_name(os.path.basename(path))[0]
+    rp, col, _, M = cases.CASES[name]()
+    tol = 2.0 ** -9
+    if "C_run" in g.files:
+        bound = O.spmm_absbound_f64(rp, col, None, M, g["B"])
+        c64 = O.spmm_f64(rp, col, None, M, g["B"])
+        assert (np.abs(g["C_run"] - c64) <= tol * bound + 1e-6).all()
+        assert (np.abs(g["C_balance"] / 1000.0 - c64) <= (tol + 1e-4) * bound + 1e-5).all()
+    if "C_run128" in g.files:
+        B = make_golden.b128(M)
+        assert B.astype(np.float64).sum() == float(g["B128_sum"])
+        rows = g["rows128"]
+        bound = O.spmm_absbound_f64(rp, col, None, M, B)[rows]
+        c64 = O.spmm_f64(rp, col, None, M, B)[rows]
+        assert (np.abs(g["C_run128"] - c64) <= tol * bound + 1e-6).all()
+        assert (np.abs(g["C_balance128"] / 1000.0 - c64) <= (tol + 1e-4) * bound + 1e-5).all()

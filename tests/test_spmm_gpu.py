@@ -120,10 +120,13 @@ def test_against_reference_spmm_golden(cuda, name):
     if not os.path.exists(path):
         pytest.skip("no reference golden vector")
     g = np.load(path)
-    if "C_run" not in g.files:
+    if "C_run" not in g.files and "C_run128" not in g.files:
         pytest.skip("reference SpMM not run on this case (num_nodes % 16 != 0)")
     rp, col, _, M = cases.CASES[name]()
     m = metcf.convert(rp, col, M)
+    if "C_run" not in g.files:
+        _check_reference_n128(m, rp, col, M, g)
+        return
     Bt = torch.from_numpy(g["B"]).cuda()
     bound = O.spmm_absbound_f64(rp, col, None, M, g["B"])
     # The reference's balance launcher runs its atomicAdd-flushing kernel
@@ -137,6 +140,31 @@ def test_against_reference_spmm_golden(cuda, name):
         assert (np.abs(o - g["C_run"]) <= 2 * TF32_TOL * bound + 1e-6).all(), "C_run"
         assert (np.abs(o - ref_balance) <= (2 * TF32_TOL + 1e-4) * bound + 1e-5).all(), \
             "C_balance"
+    if "C_run128" not in g.files:
+        return
+    _check_reference_n128(m, rp, col, M, g)
+
+
+def _check_reference_n128(m, rp, col, M, g):
+    """N = 128 through the reference's float4_split plans, against both of ours
+    and the FP64 product, on the rows the golden file keeps."""
+    import torch
+    from dtc_b200 import metcf
+    from tests.golden import make_golden
+    B = make_golden.b128(M)
+    assert B.astype(np.float64).sum() == float(g["B128_sum"]), "B128 generator changed"
+    rows = g["rows128"]
+    Bt = torch.from_numpy(B).cuda()
+    bound = O.spmm_absbound_f64(rp, col, None, M, B)[rows]
+    c64 = O.spmm_f64(rp, col, None, M, B)[rows]
+    ref_balance = g["C_balance128"].astype(np.float64) / 1000.0
+    assert (np.abs(g["C_run128"] - c64) <= TF32_TOL * bound + 1e-6).all(), "reference C_run128"
+    for ours in (metcf.spmm(m, Bt), metcf.spmm_balance(m, Bt)):
+        o = ours.cpu().numpy().astype(np.float64)[rows]
+        assert (np.abs(o - c64) <= TF32_TOL * bound + 1e-6).all(), "ours vs FP64"
+        assert (np.abs(o - g["C_run128"]) <= 2 * TF32_TOL * bound + 1e-6).all(), "C_run128"
+        assert (np.abs(o - ref_balance) <= (2 * TF32_TOL + 1e-4) * bound + 1e-5).all(), \
+            "C_balance128"
 
 
 def test_extension_api_matches_c_abi(cuda):
@@ -207,3 +235,45 @@ def test_gcn_entry_bias_relu(cuda):
     (P,) = DTCSpMM.DTCSpMM_gcn(X, m.RowWindowOffset, m.TCblocktileId, m.TCblockoffset,
                                m.SparseAToX, M, len(col))
     torch.testing.assert_close(C, torch.relu(P + b), rtol=0, atol=1e-6)
+
+
+def test_rowid_to_window_offset_matches_conversion(cuda):
+    import ctypes as C
+    import torch
+    from dtc_b200 import _lib, metcf
+    rp, col, val, M = cases.empty_windows()
+    m = metcf.convert(rp, col, M, values=val)
+    rwo = torch.full((m.nwin + 1,), -7, dtype=torch.int32, device="cuda")
+    rc = _lib.lib().dtc_rowid_to_window_offset(
+        C.c_void_p(m.TCblockRowid.data_ptr()), C.c_int64(m.T), m.nwin, C.c_void_p(rwo.data_ptr()),
+        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    assert torch.equal(rwo, m.RowWindowOffset)
+    assert metcf.device_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("bad", ["too_large", "negative", "descending"])
+def test_rowid_to_window_offset_flags_bad_ids_and_stays_in_bounds(cuda, bad):
+    """Window ids are caller input: ids outside [0, num_windows) or out of order
+    set the device error bit for a skipped index, and the writes stay inside the
+    (num_windows + 1)-entry table (canaries on both sides stay intact)."""
+    import ctypes as C
+    import torch
+    from dtc_b200 import _lib, metcf
+    nwin, T = 10, 40
+    rowid = torch.arange(T, dtype=torch.int32, device="cuda") // 4
+    if bad == "too_large":
+        rowid[-3:] = nwin + 1000
+    elif bad == "negative":
+        rowid[:2] = -50
+    else:
+        rowid[20] = 1
+    buf = torch.full((nwin + 1 + 64,), 12345, dtype=torch.int32, device="cuda")
+    rwo = buf[32:32 + nwin + 1]
+    metcf.device_status(clear=True)
+    rc = _lib.lib().dtc_rowid_to_window_offset(
+        C.c_void_p(rowid.data_ptr()), C.c_int64(T), nwin, C.c_void_p(rwo.data_ptr()),
+        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0
+    assert metcf.device_status(clear=True) & 2
+    assert (buf[:32] == 12345).all() and (buf[32 + nwin + 1:] == 12345).all()

@@ -3,9 +3,10 @@ cannot allocate device memory (graph captures, memory-budgeted servers,
 plugins without an allocator): it keeps its scratch in an array compiled into
 the library instead of a caller workspace.
 
-Called through the C ABI and compared with the regular entry point
-(dtc_spmm_balance) within the TF32 tolerance of tests/test_spmm_gpu.py, on two
-calls in a row (the second call reuses the array the first one left behind).
+Called through the C ABI and compared, within the TF32 tolerance of
+tests/test_spmm_gpu.py, with the regular entry point (dtc_spmm_balance) and
+with the FP64 product of the host oracle, on two calls in a row (the second
+call reuses the array the first one left behind).
 This file is named so that pytest collects it last; it also passes alone in a
 fresh process.
 """
@@ -43,6 +44,7 @@ def test_noalloc_matches_workspace_entry_point_twice(cuda, name, N):
     B = np.random.default_rng(9).standard_normal((M, N)).astype(np.float32)
     Bt = torch.from_numpy(B).cuda()
     ref = metcf.spmm_balance(m, Bt).cpu().numpy().astype(np.float64)
+    c64 = O.spmm_f64(rp, col, val, M, B)
     bound = O.spmm_absbound_f64(rp, col, val, M, B)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call in range(2):
@@ -51,6 +53,7 @@ def test_noalloc_matches_workspace_entry_point_twice(cuda, name, N):
         assert rc == 0, _lib.lib().dtc_last_error()
         got = out.cpu().numpy().astype(np.float64)
         assert np.isfinite(got).all()
+        assert (np.abs(got - c64) <= TF32_TOL * bound + 1e-6).all(), f"call {call} vs FP64"
         assert (np.abs(got - ref) <= TF32_TOL * bound + 1e-6).all(), f"call {call}"
     assert metcf.device_status(clear=True) == 0
 
