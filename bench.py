@@ -421,9 +421,16 @@ def run_batched(args):
     tune_s = time.perf_counter() - t0
     bs.capture()
     one_ms = timed(bs.run, args.steps, args.warmup)
+    # the same launch with one CTA per chunk (hardware block scheduler, no queue)
+    bs.queue = False
+    bs._alloc_ws()
+    bs.capture()
+    static_ms = timed(bs.run, args.steps, args.warmup)
     ms_sep, run_sep = batched.separate_launches(mats, N)
     outs = [torch.empty((m.M, N), device="cuda") for m in mats]
     sep_ms = timed(lambda: run_sep(Bt, outs), max(3, args.steps // 4), 2)
+    g_sep = batched.separate_launches_graph(ms_sep, Bt, outs)
+    sep_graph_ms = timed(g_sep.replay, max(3, args.steps // 4), 2)
     line = {"metric": "batched SpMM GFLOP/s (2*nnz*N), one graph launch vs per-matrix launches",
             "value": flops / (one_ms * 1e-3) / 1e9, "unit": "GFLOP/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": one_ms,
@@ -432,15 +439,59 @@ def run_batched(args):
             "config": {"workload": f"{args.batch} zipf(2.1) matrices, rows log-uniform "
                                    f"[256, 65536], N={N}", "nnz": int(nnz),
                        "rows": int(sum(m.M for m in mats)), "T": bs.m.T},
+            "one_cta_per_chunk_ms": static_ms,
             "separate_launches_ms": sep_ms,
             "separate_launches_gflops": flops / (sep_ms * 1e-3) / 1e9,
+            "separate_launches_one_graph_ms": sep_graph_ms,
             "speedup_vs_separate": sep_ms / one_ms,
-            "gpu_launches": (2 if bs.mode == 1 and bs.grid > 1 else 1) * args.steps,
+            "speedup_vs_separate_one_graph": sep_graph_ms / one_ms,
+            "speedup_vs_one_cta_per_chunk": static_ms / one_ms,
+            "gpu_launches": (3 if bs.mode == 1 and bs.grid > 1 else 2) * args.steps,
             "schedule": {"H": bs.m.H, "mode": bs.mode, "grid": bs.grid, "ntile": bs.ntile,
                          "autotune_ms": {h: v.ms for h, v in table.items()},
                          "autotune_s": tune_s},
             "generation_s": gen_s}
     print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------- balance report
+def run_balance_report(args):
+    """Per-CTA busy times (dtc_set_cta_timer) of one SpMM launch per schedule:
+    window mode vs strict balance, persistent CTAs on the chunk queue vs one
+    CTA per chunk; plain TF32 and the BF16X2 split form at window height 32."""
+    import torch
+    from dtc_b200 import balance, metcf, tune, B_F32, B_BF16X2, PREC_TF32, PREC_SPLIT3
+    torch.cuda.set_device(0)
+    A, Bh, N, name = make_workload(args)
+    dev = torch.device("cuda", 0)
+    B = torch.from_numpy(Bh).to(dev)
+    m = metcf.convert(A.rowptr, A.col, A.M, H=32, values=A.val, device=dev)
+    out = torch.empty((A.M, N), device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    rows = {}
+    for form, fmt, prec in (("tf32", B_F32, PREC_TF32), ("bf16x2x3", B_BF16X2, PREC_SPLIT3)):
+        planes = [B] if fmt == B_F32 else metcf.pack_b(B, fmt)
+        for mode in (0, 1):
+            grid = min(16 * sms, m.T)
+            full = metcf.spmm_ex_workspace_bytes(m, N, mode, grid)
+            for queue in (True, False):
+                wsb = full if queue else max(full - _queue_bytes(m, grid), 0)
+                ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=dev)
+                fn = lambda: metcf.spmm_ex(m, planes, fmt, N, prec, mode=mode, grid=grid,
+                                           out=out, workspace=ws if wsb else None)
+                for _ in range(3):
+                    fn()
+                r = balance.cta_report(fn, capacity=max(grid, sms) + 8, device=dev)
+                rows[f"{form}_h32_mode{mode}_{'persistent' if queue else 'one-cta-per-chunk'}"] = r
+    line = {"metric": "per-CTA busy time of one SpMM launch (us)", "workload": name,
+            "nnz": A.nnz, "T": m.T, "chunks": min(16 * sms, m.T), "schedules": rows}
+    print(json.dumps(line), flush=True)
+
+
+def _queue_bytes(m, grid):
+    """Bytes of the chunk-queue region spmm_ex_workspace_bytes includes."""
+    from dtc_b200 import metcf
+    return metcf.spmm_ex_workspace_bytes(m, 128, 0, grid)
 
 
 # ------------------------------------------------------------------ our arm
@@ -450,7 +501,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="rmat", choices=["rmat", "stencil", "uniform", "batched"])
+    ap.add_argument("--config", default="rmat",
+                    choices=["rmat", "stencil", "uniform", "batched", "balance"])
     ap.add_argument("--batch", type=int, default=512)
     ap.add_argument("--scale", type=int, default=20)
     ap.add_argument("--N", type=int, default=0)
@@ -464,6 +516,9 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.config == "batched":
         return run_batched(args)
+    if args.config == "balance":
+        args.config = "rmat"
+        return run_balance_report(args)
 
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -555,11 +610,13 @@ def main():
         results[k] = {"ms": ms, "gflops": flops / (ms * 1e-3) / 1e9,
                       "hbm_frac": nbytes / (float(np.mean(per)) * 1e-3) / 1e9 / peaks["hbm_gbs"],
                       "bytes_per_B_elem": eb}
-    # autotuned schedules: every (mode, waves, N-tile) at window heights 16 and 32 for the
-    # plain TF32 drop-in and for the two B forms within 1e-5 (dtc_autotune, CUDA events)
+    # autotuned schedules: every (mode, chunks, N-tile) at block shapes 16 x 8, 32 x 8 and
+    # 16 x 16 for the plain TF32 drop-in and for the two B forms within 1e-5 (dtc_autotune)
     from dtc_b200 import tune, costmodel, reorder as reorder_mod
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    mets = {16: m, 32: metcf.convert(A.rowptr, A.col, A.M, H=32, values=A.val, device=dev)}
+    mets = {(16, 8): m,
+            (32, 8): metcf.convert(A.rowptr, A.col, A.M, H=32, values=A.val, device=dev),
+            (16, 16): metcf.convert(A.rowptr, A.col, A.M, H=16, W=16, values=A.val, device=dev)}
     tuned_tbl = {}
     for H, mm in mets.items():
         ws_t = tune.workspace_for(mm, N, dev)
@@ -571,6 +628,7 @@ def main():
             tuned_tbl[(fo, H)] = best
         del ws_t
     plain_key = min((k for k in tuned_tbl if k[0] == "tf32"), key=lambda k: tuned_tbl[k].ms)
+    shape_name = lambda hw: f"h{hw[0]}w{hw[1]}"
     exh_key = min((k for k in tuned_tbl if k[0] != "tf32"), key=lambda k: tuned_tbl[k].ms)
 
     # the learned scheduler's choice (features -> MLP on the GPU, its 4 cheapest
@@ -590,13 +648,14 @@ def main():
                                                 torch.from_numpy(A.val).to(dev), A.M)
         torch.cuda.synchronize()
         tca_s = time.perf_counter() - t0
-        mt = metcf.convert(rp2, c2, A.M, H=plan.H, values=v2, device=dev)
+        mt = metcf.convert(rp2, c2, A.M, H=plan.H, W=getattr(plan, "W", 8), values=v2,
+                           device=dev)
         At = type("CSR", (), dict(rowptr=rp2.cpu().numpy(), col=c2.cpu().numpy(),
                                   val=v2.cpu().numpy(), M=A.M, K=A.K, nnz=A.nnz))
         Bt = B.index_select(0, perm.long()).contiguous()
     else:
         tca_s = 0.0
-        mt = mets[plan.H]
+        mt = mets[(plan.H, getattr(plan, "W", 8))]
         Bt = B
     fmt_t, prec_t, eb_t = tune.FORMS[plan.form][0], tune.FORMS[plan.form][1], \
         tune.FORMS[plan.form][2]
@@ -606,8 +665,8 @@ def main():
     ws_m = tune.workspace_for(mt, N, dev)
     out_t = out_for("tuned")
     tuned_fn = lambda: tune.run(mt, planes_t, fmt_t, N, prec_t, sched, out=out_t, workspace=ws_m)
-    tuned = f"{plan.form}_h{plan.H}_mode{plan.mode}_w{plan.waves}_nt{plan.ntile}" + \
-        ("_tca" if plan.reorder else "")
+    tuned = f"{plan.form}_{shape_name((mt.H, mt.W))}_mode{plan.mode}_w{plan.waves}" + \
+        f"_nt{plan.ntile}" + ("_tca" if plan.reorder else "")
     launches = metcf.spmm_ex_launches(mt, sched.mode, sched.grid)
 
     # the plain TF32 drop-in at its autotuned schedule, timed like the headline
@@ -636,7 +695,7 @@ def main():
     for _ in range(3):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        metcf.convert(rp_t, col_t, A.M, H=plan.H, values=val_t, device=dev)
+        metcf.convert(rp_t, col_t, A.M, H=mt.H, W=mt.W, values=val_t, device=dev)
         torch.cuda.synchronize()
         conv.append((time.perf_counter() - t0) * 1e3)
     conv16 = []
@@ -689,15 +748,16 @@ def main():
            "steps": e2e_steps, "api": "dtc_b200.hostpipe.HostPipeline (pack_b + spmm_ex)"}
     learned = {"class": costmodel.CLASSES[plan.cls], "source": plan.source,
                "plan_s": plan_s, "tca_reorder_s": tca_s, "T": mt.T, "ms": kern_ms,
-               "exhaustive_no_reorder": {"form": exh_key[0], "H": exh_key[1],
+               "exhaustive_no_reorder": {"form": exh_key[0], "shape": shape_name(exh_key[1]),
                                          "mode": tuned_tbl[exh_key].mode,
                                          "waves": tuned_tbl[exh_key].waves,
                                          "ntile": tuned_tbl[exh_key].ntile,
                                          "ms": tuned_tbl[exh_key].ms},
-               "plain_tf32_tuned": {"H": plain_key[1], "mode": sp.mode, "waves": sp.waves,
+               "plain_tf32_tuned": {"shape": shape_name(plain_key[1]), "mode": sp.mode,
+                                    "waves": sp.waves,
                                     "ntile": sp.ntile, "ms": plain_ms,
                                     "autotune_ms": tuned_tbl[plain_key].ms},
-               "autotune": {f"{k[0]}_h{k[1]}": v.ms for k, v in tuned_tbl.items()}}
+               "autotune": {f"{k[0]}_{shape_name(k[1])}": v.ms for k, v in tuned_tbl.items()}}
     tf32_best = min(("tf32_window", "tf32_balance"), key=lambda k: results[k]["ms"])
 
     cpu, errs = (None, {})
@@ -725,8 +785,8 @@ def main():
                 "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic",
                 "config": {"workload": name, "num_nodes": A.M, "nnz": A.nnz, "N": N,
-                           "T": mt.T, "form": tuned, "plain_form": "tf32_h%d (autotuned)"
-                           % plain_key[1],
+                           "T": mt.T, "form": tuned,
+                           "plain_form": f"tf32_{shape_name(plain_key[1])} (autotuned)",
                            "l2": "inputs larger than L2 (B %.0f MiB fp32, ME-TCF %.0f MB); no flush"
                            % (A.K * N * 4 / 2 ** 20, S / 1e6),
                            "timed_blocks": blocks,

@@ -15,6 +15,8 @@ std::mutex g_mu;
 int g_sms[kMaxDev] = {};
 int g_major[kMaxDev] = {};
 uint32_t* g_err_ptr[kMaxDev] = {};
+uint64_t* g_timer[kMaxDev] = {};
+int32_t g_timer_cap[kMaxDev] = {};
 
 int cur_dev() {
   int d = 0;
@@ -86,6 +88,23 @@ dtc_status encode_c_map(CUtensorMap* map, float* C, int64_t M, int32_t N, int bo
   return DTC_OK;
 }
 
+uint64_t* cta_timer_buffer(int32_t* capacity) {
+  int d = cur_dev();
+  std::lock_guard<std::mutex> lk(g_mu);
+  *capacity = g_timer_cap[d];
+  return g_timer[d];
+}
+
+// The chunk-queue region at byte `offset` of a caller workspace of `bytes`
+// bytes, or null when it does not fit (the kernels then run one CTA per chunk).
+void* queue_region(void* ws, size_t bytes, size_t offset, int64_t T, int grid) {
+  if (!ws) return nullptr;
+  const size_t need = spmm_queue_bytes(T, grid);
+  char* q = (char*)ws + offset;
+  if (((uintptr_t)q & 255) != 0 || offset + need > bytes) return nullptr;
+  return q;
+}
+
 uint32_t* device_error_word() {
   int d = cur_dev();
   std::lock_guard<std::mutex> lk(g_mu);
@@ -116,6 +135,16 @@ dtc_status dtc_device_status(uint32_t* flags, int clear) {
   DTC_CUDA(cudaDeviceSynchronize());
   DTC_CUDA(cudaMemcpy(flags, p, 4, cudaMemcpyDeviceToHost));
   if (clear) DTC_CUDA(cudaMemset(p, 0, 4));
+  return DTC_OK;
+}
+
+dtc_status dtc_set_cta_timer(uint64_t* d_records, int32_t capacity) {
+  DTC_REQUIRE(capacity >= 0, "capacity must be >= 0");
+  DTC_REQUIRE(capacity == 0 || d_records != nullptr, "null record buffer");
+  int d = cur_dev();
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_timer[d] = capacity > 0 ? d_records : nullptr;
+  g_timer_cap[d] = capacity;
   return DTC_OK;
 }
 
@@ -150,7 +179,8 @@ dtc_status dtc_spmm_balance_workspace_bytes(int32_t num_nodes, int64_t num_block
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
   int32_t nwin = (num_nodes + 15) / 16;
-  *bytes = align_up((size_t)(nwin + 1) * 4, 256) + spmm_partials_bytes(num_blocks, N, 0);
+  *bytes = align_up((size_t)(nwin + 1) * 4, 256) + align_up(spmm_partials_bytes(num_blocks, N, 0), 256) +
+           spmm_queue_bytes(num_blocks, 0);
   return DTC_OK;
 }
 
@@ -159,27 +189,28 @@ dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tile
                             const float* d_tcValues, int32_t num_nodes, int64_t num_blocks,
                             const float* d_B, int32_t N, float* d_C, void* d_workspace,
                             size_t workspace_bytes, dtc_stream_t stream) {
-  size_t need = 0;
-  dtc_status s = dtc_spmm_balance_workspace_bytes(num_nodes, num_blocks, N, &need);
-  if (s != DTC_OK) return s;
+  DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
   DTC_REQUIRE(d_tcblockOffset && d_B && d_C, "null device pointer");
   DTC_REQUIRE(num_blocks == 0 || (d_tcblockRowid && d_tileId && d_sparseAToX),
               "null device pointer");
-  if (!d_workspace || workspace_bytes < need) {
-    set_error("balance workspace too small");
+  int32_t nwin = (num_nodes + 15) / 16;
+  const size_t rwo_bytes = align_up((size_t)(nwin + 1) * 4, 256);
+  const size_t part_bytes = align_up(spmm_partials_bytes(num_blocks, N, 0), 256);
+  if (!d_workspace || workspace_bytes < rwo_bytes + part_bytes) {
+    set_error("balance workspace too small (dtc_spmm_balance_workspace_bytes)");
     return DTC_ERR_WORKSPACE_TOO_SMALL;
   }
   cudaStream_t st = (cudaStream_t)stream;
-  int32_t nwin = (num_nodes + 15) / 16;
   int32_t* rwo = (int32_t*)d_workspace;
-  float* part = (float*)((char*)d_workspace + align_up((size_t)(nwin + 1) * 4, 256));
-  s = rowid_to_rwo(d_tcblockRowid, num_blocks, nwin, rwo, st);
+  float* part = (float*)((char*)d_workspace + rwo_bytes);
+  void* queue = queue_region(d_workspace, workspace_bytes, rwo_bytes + part_bytes, num_blocks, 0);
+  dtc_status s = rowid_to_rwo(d_tcblockRowid, num_blocks, nwin, rwo, st);
   if (s != DTC_OK) return s;
   if (N % 4 != 0)
     return spmm_mma_sync_impl(rwo, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
                               num_nodes, nwin, d_B, N, d_C, st);
   return spmm_tf32_impl(rwo, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues, num_nodes,
-                        nwin, num_blocks, d_B, N, d_C, 1, 0, part, st);
+                        nwin, num_blocks, d_B, N, d_C, 1, 0, part, st, 0, Epilogue{}, 16, queue);
 }
 
 dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
@@ -187,7 +218,8 @@ dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, in
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
   DTC_REQUIRE(block_h == 16 || block_h == 32, "block_h must be 16 or 32");
-  *bytes = (mode == 1) ? spmm_partials_bytes(num_blocks, N, grid, block_h) : 0;
+  *bytes = ((mode == 1) ? align_up(spmm_partials_bytes(num_blocks, N, grid, block_h), 256) : 0) +
+           spmm_queue_bytes(num_blocks, grid);
   return DTC_OK;
 }
 
@@ -197,25 +229,28 @@ namespace {
 
 dtc_status spmm_ex_impl(const int32_t* rwo, const uint8_t* tile, const int32_t* toff,
                         const int32_t* s2x, const float* vals, int32_t M, int32_t nwin, int64_t T,
-                        int32_t H, int bformat, const void* p0, const void* p1, int32_t N,
+                        int32_t H, int32_t W, int bformat, const void* p0, const void* p1, int32_t N,
                         int precision, float* C, int mode, int grid, int ntile, Epilogue epi,
                         void* ws, size_t wsb, cudaStream_t st) {
   DTC_REQUIRE(mode == 0 || mode == 1, "mode must be 0 (window) or 1 (balance)");
   DTC_REQUIRE(grid >= 0, "grid must be >= 0");
   DTC_REQUIRE(ntile == 0 || ntile == 1 || ntile == 2 || ntile == 4, "ntile must be 0, 1, 2 or 4");
   DTC_REQUIRE(rwo && toff && p0 && C, "null device pointer");
-  size_t need = 0;
-  dtc_status s = dtc_spmm_ex_workspace_bytes(M, T, N, H, mode, grid, &need);
-  if (s != DTC_OK) return s;
-  if (need > 0 && (!ws || wsb < need)) {
-    set_error("spmm workspace too small");
+  DTC_REQUIRE(M >= 0 && T >= 0 && N >= 1, "bad sizes");
+  DTC_REQUIRE(H == 16 || H == 32, "block_h must be 16 or 32");
+  // required: the partial tiles of balance mode; optional after them: the
+  // chunk queue (persistent CTAs)
+  const size_t part_bytes = (mode == 1) ? align_up(spmm_partials_bytes(T, N, grid, H), 256) : 0;
+  if (part_bytes > 0 && (!ws || wsb < part_bytes)) {
+    set_error("spmm workspace too small (dtc_spmm_ex_workspace_bytes)");
     return DTC_ERR_WORKSPACE_TOO_SMALL;
   }
+  void* queue = queue_region(ws, wsb, part_bytes, T, grid);
   if (bformat == DTC_B_F32 && precision == DTC_PREC_TF32)
     return spmm_tf32_impl(rwo, tile, toff, s2x, vals, M, nwin, T, (const float*)p0, N, C, mode,
-                          grid, (float*)ws, st, ntile, epi, H);
+                          grid, (float*)ws, st, ntile, epi, H, queue, W);
   return spmm_split_impl(rwo, tile, toff, s2x, vals, M, nwin, T, bformat, p0, p1, N, precision,
-                         C, mode, grid, (float*)ws, st, ntile, epi, H);
+                         C, mode, grid, (float*)ws, st, ntile, epi, H, queue, W);
 }
 
 }  // namespace
@@ -225,12 +260,13 @@ extern "C" {
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                       int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
-                       const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
-                       int grid, int ntile, void* d_workspace, size_t workspace_bytes,
-                       dtc_stream_t stream) {
+                       int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                       const void* d_Bplane0, const void* d_Bplane1, int32_t N, int precision,
+                       float* d_C, int mode, int grid, int ntile, void* d_workspace,
+                       size_t workspace_bytes, dtc_stream_t stream) {
   return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
-                      num_nodes, num_windows, num_blocks, block_h, bformat, d_Bplane0, d_Bplane1, N,
+                      num_nodes, num_windows, num_blocks, block_h, block_w, bformat, d_Bplane0,
+                      d_Bplane1, N,
                       precision, d_C, mode, grid, ntile, Epilogue{}, d_workspace,
                       workspace_bytes, (cudaStream_t)stream);
 }
@@ -238,16 +274,18 @@ dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId
 dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                           const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                           const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                          int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
-                          const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
+                          int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                          const void* d_Bplane0, const void* d_Bplane1, int32_t N,
+                          int precision, const float* d_bias,
                           int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
                           size_t workspace_bytes, dtc_stream_t stream) {
   Epilogue e;
   e.bias = d_bias;
   e.relu = relu != 0;
   return spmm_ex_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX, d_tcValues,
-                      num_nodes, num_windows, num_blocks, block_h, bformat, d_Bplane0, d_Bplane1,
-                      N, precision, d_C, mode, grid, ntile, e, d_workspace, workspace_bytes,
+                      num_nodes, num_windows, num_blocks, block_h, block_w, bformat, d_Bplane0,
+                      d_Bplane1, N, precision, d_C, mode, grid, ntile, e, d_workspace,
+                      workspace_bytes,
                       (cudaStream_t)stream);
 }
 

@@ -37,6 +37,14 @@ enum : uint32_t {
 };
 uint32_t* device_error_word();  // device address of the word (per device)
 
+// Per-CTA timer buffer of the current device set by dtc_set_cta_timer (null
+// when off); *capacity receives its size in CTA records.
+uint64_t* cta_timer_buffer(int32_t* capacity);
+
+// The chunk-queue region at byte `offset` of a caller workspace, or null when it
+// does not fit or is not 256-byte aligned.
+void* queue_region(void* ws, size_t bytes, size_t offset, int64_t T, int grid);
+
 // Aligns a workspace carve-out.
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

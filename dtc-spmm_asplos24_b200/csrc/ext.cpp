@@ -134,11 +134,23 @@ std::vector<torch::Tensor> run_DTCSpMM(torch::Tensor X, torch::Tensor RowWindowO
                             TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(), vp,
                             (int32_t)num_nodes, nwin, X.data_ptr<float>(), (int32_t)X.size(1),
                             C.data_ptr<float>(), cur_stream()), "dtc_spmm_mma_sync");
-  } else {
+  } else if (X.size(1) % 4 != 0) {
     check(dtc_spmm(RowWindowOffset.data_ptr<int32_t>(), TCblocktileId.data_ptr<uint8_t>(),
                    TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(), vp,
                    (int32_t)num_nodes, nwin, T, X.data_ptr<float>(), (int32_t)X.size(1),
                    C.data_ptr<float>(), cur_stream()), "dtc_spmm");
+  } else {
+    // the window-scheduled product with the chunk queue in a torch workspace
+    const int32_t N = (int32_t)X.size(1);
+    size_t wsb = 0;
+    check(dtc_spmm_ex_workspace_bytes((int32_t)num_nodes, T, N, 16, 0, 0, &wsb),
+          "dtc_spmm_ex_workspace_bytes");
+    auto ws = torch::empty({(int64_t)(wsb > 0 ? wsb : 1)}, X.options().dtype(torch::kUInt8));
+    check(dtc_spmm_ex(RowWindowOffset.data_ptr<int32_t>(), TCblocktileId.data_ptr<uint8_t>(),
+                      TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(), vp,
+                      (int32_t)num_nodes, nwin, T, 16, 8, DTC_B_F32, X.data_ptr<float>(), nullptr,
+                      N, DTC_PREC_TF32, C.data_ptr<float>(), 0, 0, 0, ws.data_ptr(), wsb,
+                      cur_stream()), "dtc_spmm_ex");
   }
   return {C};
 }
@@ -168,11 +180,16 @@ std::vector<torch::Tensor> DTCSpMM_gcn(torch::Tensor X, torch::Tensor RowWindowO
   auto C = torch::empty_like(X);
   const int32_t nwin = (int32_t)RowWindowOffset.numel() - 1;
   const int64_t T = TCblockoffset.numel() - 1;
+  size_t wsb = 0;
+  check(dtc_spmm_ex_workspace_bytes((int32_t)num_nodes, T, N, 16, 0, 0, &wsb),
+        "dtc_spmm_ex_workspace_bytes");
+  auto ws = torch::empty({(int64_t)(wsb > 0 ? wsb : 1)}, X.options().dtype(torch::kUInt8));
   check(dtc_spmm_fused(RowWindowOffset.data_ptr<int32_t>(), TCblocktileId.data_ptr<uint8_t>(),
                        TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(),
                        values_ptr(values, TCblocktileId.numel()), (int32_t)num_nodes, nwin, T, 16,
-                       DTC_B_F32, X.data_ptr<float>(), nullptr, N, DTC_PREC_TF32, bp, relu ? 1 : 0,
-                       C.data_ptr<float>(), 0, 0, 0, nullptr, 0, cur_stream()),
+                       8, DTC_B_F32, X.data_ptr<float>(), nullptr, N, DTC_PREC_TF32, bp,
+                       relu ? 1 : 0, C.data_ptr<float>(), 0, 0, 0, ws.data_ptr(), wsb,
+                       cur_stream()),
         "dtc_spmm_fused");
   return {C};
 }
@@ -212,7 +229,7 @@ std::vector<torch::Tensor> run_DTCSpMM_ex(std::vector<torch::Tensor> Bplanes, in
                                           torch::Tensor SparseAToX, int64_t num_nodes,
                                           int64_t precision, int64_t mode, int64_t grid,
                                           c10::optional<torch::Tensor> values, int64_t ntile,
-                                          int64_t block_h) {
+                                          int64_t block_h, int64_t block_w) {
   TORCH_CHECK(!Bplanes.empty(), "Bplanes is empty");
   for (auto& t : Bplanes) { CHECK_INPUT(t); }
   const c10::cuda::CUDAGuard guard(Bplanes[0].device());
@@ -227,7 +244,7 @@ std::vector<torch::Tensor> run_DTCSpMM_ex(std::vector<torch::Tensor> Bplanes, in
   check(dtc_spmm_ex(RowWindowOffset.data_ptr<int32_t>(), TCblocktileId.data_ptr<uint8_t>(),
                     TCblockoffset.data_ptr<int32_t>(), SparseAToX.data_ptr<int32_t>(),
                     values_ptr(values, TCblocktileId.numel()), (int32_t)num_nodes, nwin, T,
-                    (int32_t)block_h, (int)bformat, Bplanes[0].data_ptr(),
+                    (int32_t)block_h, (int32_t)block_w, (int)bformat, Bplanes[0].data_ptr(),
                     Bplanes.size() > 1 ? Bplanes[1].data_ptr() : nullptr, (int32_t)N,
                     (int)precision, C.data_ptr<float>(), (int)mode, (int)grid, (int)ntile,
                     ws.data_ptr(), wsb, cur_stream()), "dtc_spmm_ex");
@@ -285,7 +302,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("Bplanes"), py::arg("bformat"), py::arg("N"), py::arg("RowWindowOffset"),
         py::arg("TCblocktileId"), py::arg("TCblockoffset"), py::arg("SparseAToX"),
         py::arg("num_nodes"), py::arg("precision"), py::arg("mode") = 0, py::arg("grid") = 0,
-        py::arg("values") = py::none(), py::arg("ntile") = 0, py::arg("block_h") = 16);
+        py::arg("values") = py::none(), py::arg("ntile") = 0, py::arg("block_h") = 16,
+        py::arg("block_w") = 8);
   m.def("pack_b", &pack_b, "convert fp32 B into a storage form", py::arg("B"),
         py::arg("bformat"));
 }

@@ -25,16 +25,18 @@
 // full product takes one instruction per block, like the tf32 form, while
 // gathering 3 (SPLIT24), 2 (BF16), 1 (FP8) or 4 (BF16X2) bytes per element.
 //
-// Schedule, work split and the deterministic reduction are the tf32
-// kernel's (spmm_tc.cu). Warp roles (704 threads): epilogue 0-3, UMMA
+// Schedule, work split, producer warp and the deterministic reduction are the
+// tf32 kernel's (spmm_tc.cu, spmm_sched.cuh). Warp roles: epilogue 0-3, UMMA
 // issuers 4-5, loaders 6-9 (cp.async of the planes), tile builders 10-13
-// (A_hi / A_lo tiles), converters 14-21 (wait for a stage's gathered rows,
-// rebuild the bf16 operand rows in place). A stage is released to the UMMA
-// issuers by one tile-builder and one converter arrival. Finished C tiles
-// leave through shared memory and per-warp TMA tensor stores (16 rows x 32
-// columns). At window height 32 with one N-tile, the forms that stage a
-// second plane (SPLIT24, FP8) hold 3 blocks per stage so the 32-row A tiles
-// and the staging fit in shared memory.
+// (A_hi / A_lo tiles), producer 14, and for the forms that rebuild operand
+// rows on the CUDA cores (SPLIT24, FP8) converters 15-22, which wait for a
+// stage's gathered rows and rebuild the bf16 operand rows in place (480 or
+// 736 threads). A stage is released to the UMMA issuers by the loader's
+// cp.async arrivals and the tile builder (BF16, BF16X2), or by the tile
+// builder and the converter. Finished C tiles leave through shared memory and
+// per-warp TMA tensor stores (16 rows x 32 columns). At window height 32 with
+// one N-tile, the forms that stage a second plane (SPLIT24, FP8) hold 3
+// blocks per stage so the 32-row A tiles and the staging fit in shared memory.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 #include "spmm_sched.cuh"
@@ -50,36 +52,43 @@ constexpr int kLoadWarp0 = kMmaWarp + kMmaWarps;   // warps 6-9
 constexpr int kLoadWarps = 4;
 constexpr int kTileWarp0 = kLoadWarp0 + kLoadWarps;  // warps 10-13
 constexpr int kTileWarps = 4;
-constexpr int kConvWarp0 = kTileWarp0 + kTileWarps;  // warps 14-21
+constexpr int kProdWarp = kTileWarp0 + kTileWarps;   // warp 14
+constexpr int kConvWarp0 = kProdWarp + 1;            // warps 15-22 (SPLIT24, FP8)
 constexpr int kConvWarps = 8;
-constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 704
 constexpr int kTileBytes = 4096;  // per block and 128-feature tile: 16 K rows x 128 bf16
 
 enum { kFormSplit24 = 0, kFormBF16 = 1, kFormFP8 = 2, kFormBF16X2 = 3 };
 
 // WH = row-window height; the UMMA N dimension is 2 WH (A_hi^T | A_lo^T).
-template <int FORM, int NT, int P, int S, int WH>
+// BW = TC-block width (8 or 16): a block of width 16 is two 8-slot halves,
+// each one K = 16 (hi | lo) MMA into the same accumulator.
+template <int FORM, int NT, int P, int S, int WH, int BW>
 struct SCfg {
-  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kMmaWarps == 0 &&
-                    S % kConvWarps == 0, "ownership");
-  static_assert(P * kBlkW <= 32, "one SparseAToX entry per lane");
+  static constexpr bool kConv = (FORM == kFormSplit24 || FORM == kFormFP8);
+  static constexpr int kThreads = 32 * (kConvWarp0 + (kConv ? kConvWarps : 0));
+  static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kConvWarps == 0, "ownership");
+  static_assert(kConvWarps <= kEndStages, "end markers");
+  static_assert(BW == 8 || BW == 16, "block width");
+  static_assert(P * BW <= 32, "one SparseAToX entry per lane");
+  static_assert(WH * BW <= 256, "tile ids are bytes");
   static_assert(WH == 16 || WH == 32, "window height");
   static_assert(NT * WH <= 64, "TMEM budget: two accumulator sets per issuer");
   static constexpr int kAccCols = NT * 2 * WH;  // TMEM columns of one accumulator set
   static constexpr int kNacc = 512 / (kMmaWarps * kAccCols) < 4 ? 512 / (kMmaWarps * kAccCols) : 4;
-  static constexpr int kYB = 64 * WH;  // 16 K x 2WH N bf16, K-major core matrices
-  static constexpr int kStageX = P * NT * kTileBytes;
+  static constexpr int kSub = BW / 8;  // 8-slot halves per block
+  static constexpr int kYB8 = 64 * WH;  // 16 K x 2WH N bf16, K-major core matrices
+  static constexpr int kYB = kSub * kYB8;  // one block's A^T tile
+  static constexpr int kStageX = P * NT * kSub * kTileBytes;
   static constexpr int kRowStage = NT * 128;  // staged bytes of one gathered row (u8 / e4m3)
-  static constexpr int kStageE =
-      (FORM == kFormBF16 || FORM == kFormBF16X2) ? 0 : P * kBlkW * kRowStage;
+  static constexpr int kStageE = kConv ? P * BW * kRowStage : 0;
   static constexpr int kStageY = P * kYB;
   static constexpr int kX = S * kStageX;
   static constexpr int kE = S * kStageE;
   static constexpr int kY = S * kStageY;
-  static constexpr int kBars = (3 * S + 2 * kNacc) * 8;
+  static constexpr int kBars = (3 * S + 2 * kNacc + kMmaWarps) * 8;
   static constexpr int kStgW = 16 * 32 * 4;          // one epilogue warp's 16-row C tile
   static constexpr int kStg = kEpiWarps * 2 * kStgW;  // double-buffered per warp
-  static constexpr int kSmem = kX + kE + kY + kStg + kBars + 16 + 1024;
+  static constexpr int kSmem = kX + kE + kY + kStg + kSchedBytes + kBars + 16 + 1024;
   static constexpr int kCols = kMmaWarps * kNacc * kAccCols;
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
@@ -105,44 +114,51 @@ __device__ __forceinline__ uint16_t bf16_bits(float x) {
   return __bfloat16_as_ushort(__float2bfloat16_rn(x));
 }
 
-template <int FORM, int NT, int P, int S, bool FOUR, int WH>
-__global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constant__ Params p) {
-  using K = SCfg<FORM, NT, P, S, WH>;
+template <int FORM, int NT, int P, int S, bool FOUR, int WH, int BW>
+__global__ void __launch_bounds__(SCfg<FORM, NT, P, S, WH, BW>::kThreads, 1)
+    k_spmm_split(const __grid_constant__ Params p) {
+  using K = SCfg<FORM, NT, P, S, WH, BW>;
+  const uint64_t t_entry = global_timer_ns();
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint8_t* xring = smem;
   uint8_t* ering = smem + K::kX;
   uint8_t* yring = ering + K::kE;
   uint8_t* stg = yring + K::kY;  // [4 warps][2][16 x 32] fp32 C staging
-  uint64_t* bars = (uint64_t*)(stg + K::kStg);
-  uint64_t* loaded = bars;               // [S] 32 cp.async arrivals
-  uint64_t* full = bars + S;             // [S] 1 tile-builder + 1 converter arrival
-  uint64_t* empty = bars + 2 * S;        // [S] UMMA commit
+  const SchedRings rings = carve_rings(stg + K::kStg);
+  uint64_t* bars = (uint64_t*)(stg + K::kStg + kSchedBytes);
+  uint64_t* loaded = bars;               // [S] 32 cp.async arrivals (converter forms)
+  uint64_t* full = bars + S;             // [S] see the header comment
+  uint64_t* empty = bars + 2 * S;        // [S] the owning issuer's UMMA commit
   uint64_t* acc_full = bars + 3 * S;     // [kNacc] one commit per issuer
   uint64_t* acc_empty = acc_full + K::kNacc;
-  uint32_t* tmem_slot = (uint32_t*)(acc_empty + K::kNacc);
+  uint64_t* drain = acc_empty + K::kNacc;     // [kMmaWarps] an issuer's last commit
+  uint32_t* tmem_slot = (uint32_t*)(drain + kMmaWarps);
   volatile uint32_t* abort_flag = tmem_slot + 1;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = blockIdx.x;
   const int col0 = blockIdx.y * NT * 128;
   const int ncols = (p.N - col0) < NT * 128 ? (p.N - col0) : NT * 128;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
       mbar_init(&loaded[i], 32);
-      mbar_init(&full[i], 2);
-      mbar_init(&empty[i], 1);
+      mbar_init(&full[i], K::kConv ? 2 : 32 + 1);
+      mbar_init(&empty[i], 1);  // the owning issuer's MMA commit
     }
     for (int i = 0; i < K::kNacc; ++i) {
       mbar_init(&acc_full[i], kMmaWarps);
       mbar_init(&acc_empty[i], kEpiWarps);
     }
+    for (int i = 0; i < kMmaWarps; ++i) mbar_init(&drain[i], 1);
+    // metadata: loader + tile builder (+ converter); records: every epilogue
+    // warp and issuer
+    init_rings(rings, K::kConv ? 3 : 2, kEpiWarps + kMmaWarps);
     *abort_flag = 0;
     fence_mbar_init();
   }
   if (FORM == kFormBF16 || FORM == kFormFP8) {  // lo rows stay zero for one-plane forms
-    for (int i = threadIdx.x; i < S * P * NT; i += blockDim.x) {
+    for (int i = threadIdx.x; i < S * P * NT * K::kSub; i += blockDim.x) {  // every block tile
       float4* lo = reinterpret_cast<float4*>(xring + (size_t)i * kTileBytes + 2048);
       for (int z = 0; z < 2048 / 16; ++z) lo[z] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -157,31 +173,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  int64_t b0, b1;
-  cta_range(p, c, b0, b1);
-  const int64_t nblk = b1 - b0;
-  const int64_t nstage = (nblk + P - 1) / P;
-
-  if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
+  if (warp == kProdWarp) {
+    produce<P, BW>(p, rings, lane, abort_flag);
+  } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ------------------------------------------------------------ loaders
     const int lw = warp - kLoadWarp0;
-    auto row_of = [&](int64_t st) -> int32_t {
-      const int64_t b = b0 + st * P + (lane >> 3);
-      return (lane < P * kBlkW && st < nstage && b < b1) ? __ldg(p.s2x + b * kBlkW + (lane & 7))
-                                                         : 0;
-    };
     __shared__ int32_t rows_sm[kLoadWarps][32];  // SparseAToX of the stage being loaded
     const uint8_t* plane0 = reinterpret_cast<const uint8_t*>(p.B);
     const uint8_t* plane1 = reinterpret_cast<const uint8_t*>(p.B1);
-    int32_t rows = row_of(lw);
-    for (int64_t st = lw; st < nstage; st += kLoadWarps) {
+    for (int64_t st = lw;; st += kLoadWarps) {
+      const int ms = (int)(st % kMetaDepth);
+      if (!warp_wait(&rings.meta_full[ms], (uint32_t)(st / kMetaDepth) & 1, p.err, abort_flag))
+        break;
+      const int nb = rings.meta[ms].nb;
+      const int32_t rows = rings.meta[ms].s2x[lane];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&rings.meta_empty[ms]);
+      if (nb < 0) break;
       const int s = (int)(st % S);
       const uint32_t n = (uint32_t)(st / S);
-      const int32_t nxt = row_of(st + kLoadWarps);
-      const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
-      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
-      const int64_t sb = b0 + st * P;
-      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      if (!warp_wait(&empty[s], (n & 1) ^ 1, p.err, abort_flag)) break;
       const uint32_t xs = smem_u32(xring + (size_t)s * K::kStageX);
       const uint32_t es = smem_u32(ering + (size_t)s * K::kStageE);
       const uint8_t* eplane = FORM == kFormSplit24 ? plane1 : plane0;
@@ -197,34 +208,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
             for (int pl = 0; pl < NPL; ++pl) {
               const uint8_t* base = pl ? plane1 : plane0;
 #pragma unroll
-              for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
+              for (int k0 = 0; k0 < BW; k0 += RPI) {
                 const int k = k0 + (RPI > 1 ? lane / CPR : 0);
-                const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+                const int32_t r = __shfl_sync(0xffffffffu, rows, pb * BW + k);
                 const bool pad = (k > 0 && r == 0);  // unused slot (columns ascend in a block)
                 const uint8_t* src = base + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
 #pragma unroll
                 for (int ii = 0; ii < IPR; ++ii) {
                   const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
-                  cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes +
-                                 x_offset_bf16(pl * 8 + k, cc & 15),
+                  cp_async16(xs + ((pb * NT + (cc >> 4)) * K::kSub + (k >> 3)) * kTileBytes +
+                                 x_offset_bf16(pl * 8 + (k & 7), cc & 15),
                              src + cc * 16, pad ? 0u : 16u);
                 }
               }
             }
           }
-          if (FORM == kFormSplit24 || FORM == kFormFP8) {  // u8 ext / e4m3 plane -> staging
+          if (K::kConv) {  // u8 ext / e4m3 plane -> staging
             constexpr int CPR = NT * 8, RPI = CPR >= 32 ? 1 : 32 / CPR;
             constexpr int IPR = CPR >= 32 ? CPR / 32 : 1;
 #pragma unroll
-            for (int k0 = 0; k0 < kBlkW; k0 += RPI) {
+            for (int k0 = 0; k0 < BW; k0 += RPI) {
               const int k = k0 + (RPI > 1 ? lane / CPR : 0);
-              const int32_t r = __shfl_sync(0xffffffffu, rows, pb * kBlkW + k);
+              const int32_t r = __shfl_sync(0xffffffffu, rows, pb * BW + k);
               const bool pad = (k > 0 && r == 0);
               const uint8_t* src = eplane + (int64_t)(pad ? 0 : r) * p.N + col0;
 #pragma unroll
               for (int ii = 0; ii < IPR; ++ii) {
                 const int cc = (RPI > 1 ? lane % CPR : lane) + ii * 32;
-                cp_async16(es + (pb * kBlkW + k) * K::kRowStage + cc * 16, src + cc * 16,
+                cp_async16(es + (pb * BW + k) * K::kRowStage + cc * 16, src + cc * 16,
                            pad ? 0u : 16u);
               }
             }
@@ -234,75 +245,94 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
         // partial slice: lanes flattened over (gathered row, 16-byte chunk)
         rows_sm[lw][lane] = rows;
         __syncwarp();
-        const int nrow = nb * kBlkW;
+        const int nrow = nb * BW;
         if (FORM != kFormFP8) {
           const int nck = ncols >> 3;
           constexpr int NPL = FORM == kFormBF16X2 ? 2 : 1;
           for (int idx = lane; idx < NPL * nrow * nck; idx += 32) {
             const int pl = idx / (nrow * nck), id2 = idx - pl * nrow * nck;
             const int rowi = id2 / nck, cc = id2 - rowi * nck;
-            const int k = rowi & 7, pb = rowi >> 3;
+            const int k = rowi % BW, pb = rowi / BW;
             const int32_t r = rows_sm[lw][rowi];
             const bool pad = (k > 0 && r == 0);
             const uint8_t* src = (pl ? plane1 : plane0) + ((int64_t)(pad ? 0 : r) * p.N + col0) * 2;
-            cp_async16(xs + (pb * NT + (cc >> 4)) * kTileBytes + x_offset_bf16(pl * 8 + k, cc & 15),
+            cp_async16(xs + ((pb * NT + (cc >> 4)) * K::kSub + (k >> 3)) * kTileBytes +
+                           x_offset_bf16(pl * 8 + (k & 7), cc & 15),
                        src + cc * 16, pad ? 0u : 16u);
           }
         }
-        if (FORM == kFormSplit24 || FORM == kFormFP8) {
+        if (K::kConv) {
           const int nck = ncols >> 4;
           for (int idx = lane; idx < nrow * nck; idx += 32) {
             const int rowi = idx / nck, cc = idx - rowi * nck;
             const int32_t r = rows_sm[lw][rowi];
-            const bool pad = ((rowi & 7) > 0 && r == 0);
+            const bool pad = ((rowi % BW) > 0 && r == 0);
             const uint8_t* src = eplane + (int64_t)(pad ? 0 : r) * p.N + col0;
             cp_async16(es + rowi * K::kRowStage + cc * 16, src + cc * 16, pad ? 0u : 16u);
           }
         }
         __syncwarp();
       }
-      cp_async_arrive_noinc(&loaded[s]);
-      rows = nxt;
+      cp_async_arrive_noinc(K::kConv ? &loaded[s] : &full[s]);
     }
+    cp_async_wait_all();
   } else if (warp >= kTileWarp0 && warp < kTileWarp0 + kTileWarps) {
     // ------------------------------------------------------ tile builders
     const int tw = warp - kTileWarp0;
-    auto offs_of = [&](int64_t st) -> int32_t {
-      const int64_t sb = b0 + st * P;
-      return (st < nstage && lane <= P && sb + lane <= b1) ? __ldg(p.toff + sb + lane) : 0;
+    // One stage's prefetched inputs: its offsets (lane k holds
+    // TCblockoffset[sb + k]), block count (-1: end of work, -2: not fetched
+    // yet), and the tile ids / values of its first 64 entries.
+    struct Pf {
+      int32_t offv;
+      int nb;
+      uint32_t t0, t1;
+      float v0, v1;
     };
-    // Tile ids and values of the first 64 entries of a stage are loaded one
-    // owned stage ahead (offsets two ahead), so their global-load latency
-    // overlaps the previous stage's work instead of stalling this one.
-    int32_t offv = offs_of(tw);
-    int32_t offn = offs_of(tw + kTileWarps);
-    uint32_t pt0 = 0, pt1 = 0;
-    float pv0 = 0.0f, pv1 = 0.0f;
-    auto fetch = [&](int64_t st, int32_t ov) {
-      const int64_t sb = b0 + st * P;
-      const int nbx = st < nstage ? (int)((b1 - sb) < P ? (b1 - sb) : P) : 0;
-      const int32_t f0 = __shfl_sync(0xffffffffu, ov, 0), f1 = __shfl_sync(0xffffffffu, ov, nbx);
+    bool ok = true;
+    // Stages ahead of the one being built are only probed, never waited for:
+    // the producer emits a stage's metadata after the window records of the
+    // stages before it, and those records may need this warp's current stage
+    // finished first.
+    auto fetch = [&](int64_t st, Pf& f, bool wait) {
+      f.nb = -2;
+      f.offv = 0;
+      f.t0 = f.t1 = 0;
+      f.v0 = f.v1 = 0.0f;
+      const int ms = (int)(st % kMetaDepth);
+      const uint32_t par = (uint32_t)(st / kMetaDepth) & 1;
+      if (!wait) {
+        if (!__all_sync(0xffffffffu, mbar_try_wait(&rings.meta_full[ms], par))) return;
+      } else if (!warp_wait(&rings.meta_full[ms], par, p.err, abort_flag)) {
+        ok = false;
+        return;
+      }
+      f.nb = rings.meta[ms].nb;
+      f.offv = (f.nb >= 0 && lane <= f.nb) ? rings.meta[ms].toff[lane] : 0;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&rings.meta_empty[ms]);
+      if (f.nb < 0) return;
+      const int32_t f0 = __shfl_sync(0xffffffffu, f.offv, 0);
+      const int32_t f1 = __shfl_sync(0xffffffffu, f.offv, f.nb);
       const int32_t e = f0 + lane;
-      pt0 = (e < f1) ? __ldg(p.tile + e) : 0u;
-      pv0 = (e < f1) ? (p.vals ? __ldg(p.vals + e) : 1.0f) : 0.0f;
-      pt1 = (e + 32 < f1) ? __ldg(p.tile + e + 32) : 0u;
-      pv1 = (e + 32 < f1) ? (p.vals ? __ldg(p.vals + e + 32) : 1.0f) : 0.0f;
+      f.t0 = (e < f1) ? __ldg(p.tile + e) : 0u;
+      f.v0 = (e < f1) ? (p.vals ? __ldg(p.vals + e) : 1.0f) : 0.0f;
+      f.t1 = (e + 32 < f1) ? __ldg(p.tile + e + 32) : 0u;
+      f.v1 = (e + 32 < f1) ? (p.vals ? __ldg(p.vals + e + 32) : 1.0f) : 0.0f;
     };
-    fetch(tw, offv);
-    for (int64_t st = tw; st < nstage; st += kTileWarps) {
+    Pf cur, n1, n2;
+    fetch(tw, cur, true);
+    if (ok && cur.nb >= 0) fetch(tw + kTileWarps, n1, false); else n1.nb = -1;
+    for (int64_t st = tw; ok && cur.nb >= 0; st += kTileWarps) {
+      // probe two stages ahead unless the next one is known to end the work
+      // (an unprobed next stage, nb == -2, still lets this one be probed)
+      if (n1.nb != -1) fetch(st + 2 * kTileWarps, n2, false); else n2.nb = -1;
       const int s = (int)(st % S);
       const uint32_t n = (uint32_t)(st / S);
-      const int32_t nxt = offs_of(st + 2 * kTileWarps);
-      const uint32_t ct0 = pt0, ct1 = pt1;
-      const float cv0 = pv0, cv1 = pv1;
-      fetch(st + kTileWarps, offn);
-      const int64_t sb = b0 + st * P;
-      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
+      const int nb = cur.nb;
       int32_t off[P + 1];
 #pragma unroll
-      for (int k = 0; k <= P; ++k) off[k] = __shfl_sync(0xffffffffu, offv, k);
-      const bool got = mbar_wait(&empty[s], (n & 1) ^ 1, p.err);
-      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      for (int k = 0; k <= P; ++k) off[k] = __shfl_sync(0xffffffffu, cur.offv, k);
+      if (!warp_wait(&empty[s], (n & 1) ^ 1, p.err, abort_flag)) break;
       uint8_t* ys = yring + (size_t)s * K::kStageY;
       for (int z = lane; z < P * K::kYB / 16; z += 32)
         reinterpret_cast<float4*>(ys)[z] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -313,18 +343,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
 #pragma unroll
         for (int q = 1; q < P; ++q) pb += (q < nb && e >= off[q]) ? 1 : 0;
         const int32_t i = (e - e0) >> 5;  // chunk of this entry
-        const uint32_t pos = i == 0 ? ct0 : i == 1 ? ct1 : __ldg(p.tile + e);
-        const float v = i == 0 ? cv0 : i == 1 ? cv1 : (p.vals ? __ldg(p.vals + e) : 1.0f);
-        if (pos >= WH * kBlkW) {
+        const uint32_t pos = i == 0 ? cur.t0 : i == 1 ? cur.t1 : __ldg(p.tile + e);
+        const float v = i == 0 ? cur.v0 : i == 1 ? cur.v1 : (p.vals ? __ldg(p.vals + e) : 1.0f);
+        if (pos >= WH * BW) {
           atomicOr(p.err, kErrBadIndex);
           continue;
         }
         if (v == 0.0f) continue;
-        const uint32_t r = pos >> 3, sl = pos & 7;
+        const uint32_t r = pos / BW, sfull = pos % BW, sl = sfull & 7;
         const __nv_bfloat16 hi = __float2bfloat16_rn(v);
         const uint16_t hb = __bfloat16_as_ushort(hi);
         const uint16_t lb = bf16_bits(v - __bfloat162float(hi));
-        uint8_t* yb = ys + pb * K::kYB;
+        uint8_t* yb = ys + pb * K::kYB + (sfull >> 3) * K::kYB8;
         *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, sl)) = hb;
         *reinterpret_cast<uint16_t*>(yb + ysplit_offset(r, 8 + sl)) = hb;
         *reinterpret_cast<uint16_t*>(yb + ysplit_offset(WH + r, sl)) = lb;
@@ -333,223 +363,253 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&full[s]);
-      offv = offn;
-      offn = nxt;
+      cur = n1;
+      n1 = n2;
+      if (cur.nb == -2) fetch(st + kTileWarps, cur, true);  // not ready when probed
     }
-  } else if (warp >= kConvWarp0) {
+  } else if (K::kConv && warp >= kConvWarp0) {
     // --------------------------------------------------------- converters
     const int cw = warp - kConvWarp0;
     __shared__ float row_scale[kConvWarps][32];  // FP8: scale of stage row (pb*8 + k)
-    auto scale_of = [&](int64_t st) -> float {
-      if (FORM != kFormFP8) return 1.0f;
-      const int64_t b = b0 + st * P + (lane >> 3);
-      if (!(lane < P * kBlkW && st < nstage && b < b1)) return 0.0f;
-      const int32_t r = __ldg(p.s2x + b * kBlkW + (lane & 7));
-      return ((lane & 7) > 0 && r == 0) ? 0.0f : __ldg(reinterpret_cast<const float*>(p.B1) + r);
+    // block count (-1: end of work, -2: not fetched yet) and (FP8) the row
+    // scale of this lane's gathered row of an owned stage, probed one owned
+    // stage ahead in the metadata ring (never waited for ahead of the stage
+    // being converted: see the tile builders)
+    bool ok = true;
+    auto meta_of = [&](int64_t st, int& nb, float& sc, bool wait) {
+      nb = -2;
+      sc = 0.0f;
+      const int ms = (int)(st % kMetaDepth);
+      const uint32_t par = (uint32_t)(st / kMetaDepth) & 1;
+      if (!wait) {
+        if (!__all_sync(0xffffffffu, mbar_try_wait(&rings.meta_full[ms], par))) return;
+      } else if (!warp_wait(&rings.meta_full[ms], par, p.err, abort_flag)) {
+        ok = false;
+        return;
+      }
+      nb = rings.meta[ms].nb;
+      const int32_t r = rings.meta[ms].s2x[lane];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&rings.meta_empty[ms]);
+      if (FORM == kFormFP8 && nb >= 0)
+        sc = (lane < nb * BW && !((lane % BW) > 0 && r == 0))
+                 ? __ldg(reinterpret_cast<const float*>(p.B1) + r) : 0.0f;
     };
-    float scv = scale_of(cw);
+    int nb_c, nb_n;
+    float sc_c, sc_n;
+    meta_of(cw, nb_c, sc_c, true);
     const int nchunk = ncols >> 3;  // 8-feature chunks per gathered row
-    for (int64_t st = cw; st < nstage; st += kConvWarps) {
+    for (int64_t st = cw; ok && nb_c >= 0; st += kConvWarps) {
+      meta_of(st + kConvWarps, nb_n, sc_n, false);
       const int s = (int)(st % S);
       const uint32_t n = (uint32_t)(st / S);
-      const float scn = scale_of(st + kConvWarps);
-      const int64_t sb = b0 + st * P;
-      const int nb = (int)((b1 - sb) < P ? (b1 - sb) : P);
-      const bool got = mbar_wait(&loaded[s], n & 1, p.err);  // implies the stage was empty
-      if (!__all_sync(0xffffffffu, got) || *abort_flag) { *abort_flag = 1; break; }
+      const int nb = nb_c;
+      if (!warp_wait(&loaded[s], n & 1, p.err, abort_flag)) break;  // implies the stage was empty
       if (FORM == kFormFP8) {
-        row_scale[cw][lane] = scv;
+        row_scale[cw][lane] = sc_c;
         __syncwarp();
       }
-      if (FORM == kFormSplit24 || FORM == kFormFP8) {
-        uint8_t* xs = xring + (size_t)s * K::kStageX;
-        const uint8_t* es = ering + (size_t)s * K::kStageE;
-        const int items = nb * kBlkW * nchunk;
-        // item it: 8 features (16 B of bf16) of gathered row rowi = pb * 8 + k
-        auto locate = [&](int it, uint32_t& xoff, uint32_t& eoff, int& rowi) {
-          rowi = nchunk == NT * 16 ? it / (NT * 16) : it / nchunk;
-          const int j = it - rowi * nchunk;
-          xoff = (uint32_t)(((rowi >> 3) * NT + (j >> 4)) * kTileBytes) +
-                 x_offset_bf16(rowi & 7, j & 15);
-          eoff = (uint32_t)(rowi * K::kRowStage + j * 8);
-        };
-        // SPLIT24: lo = b24 - hi is exact in bf16, so its bf16 bits are the
-        // top half of the fp32 difference. Per element pair: the hi bits go
-        // to the top of two fp32 words (byte permutes), the extension bytes
-        // under them, one packed fp32x2 subtraction, one permute to pack.
-        auto lo_words = [&](const uint4& h, const uint2& e, uint32_t (&o)[4]) {
-          const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
-          const uint32_t ew[2] = {e.x, e.y};
+      uint8_t* xs = xring + (size_t)s * K::kStageX;
+      const uint8_t* es = ering + (size_t)s * K::kStageE;
+      const int items = nb * BW * nchunk;
+      // item it: 8 features (16 B of bf16) of gathered row rowi = pb * BW + k
+      auto locate = [&](int it, uint32_t& xoff, uint32_t& eoff, int& rowi) {
+        rowi = nchunk == NT * 16 ? it / (NT * 16) : it / nchunk;
+        const int j = it - rowi * nchunk;
+        const int pb = rowi / BW, k = rowi % BW;
+        xoff = (uint32_t)(((pb * NT + (j >> 4)) * K::kSub + (k >> 3)) * kTileBytes) +
+               x_offset_bf16(k & 7, j & 15);
+        eoff = (uint32_t)(rowi * K::kRowStage + j * 8);
+      };
+      // SPLIT24: lo = b24 - hi is exact in bf16, so its bf16 bits are the
+      // top half of the fp32 difference. Per element pair: the hi bits go
+      // to the top of two fp32 words (byte permutes), the extension bytes
+      // under them, one packed fp32x2 subtraction, one permute to pack.
+      auto lo_words = [&](const uint4& h, const uint2& e, uint32_t (&o)[4]) {
+        const uint32_t hw[4] = {h.x, h.y, h.z, h.w};
+        const uint32_t ew[2] = {e.x, e.y};
 #pragma unroll
-          for (int z = 0; z < 4; ++z) {
-            const uint32_t eword = ew[z >> 1];
-            const uint32_t sel0 = 0x3200u | ((4u + 2u * (z & 1)) << 4);      // ext byte 2z
-            const uint32_t sel1 = 0x3200u | ((4u + 2u * (z & 1) + 1u) << 4); // ext byte 2z+1
-            const uint32_t h0 = __byte_perm(hw[z], 0u, 0x1044);
-            const uint32_t h1 = hw[z] & 0xFFFF0000u;
-            const uint32_t b0 = __byte_perm(h0, eword, sel0);
-            const uint32_t b1 = __byte_perm(h1, eword, sel1);
-            uint32_t l0, l1;
-            asm("{\n\t.reg .b64 a, b, d;\n\t"
-                "mov.b64 a, {%2, %3};\n\t"
-                "mov.b64 b, {%4, %5};\n\t"
-                "sub.rn.f32x2 d, a, b;\n\t"
-                "mov.b64 {%0, %1}, d;\n\t}"
-                : "=r"(l0), "=r"(l1)
-                : "r"(b0), "r"(b1), "r"(h0), "r"(h1));
-            o[z] = __byte_perm(l0, l1, 0x7632);
-          }
-        };
-        auto fp8_words = [&](const uint2& e, float sc, uint32_t (&o)[4]) {
-          const uint32_t ew[2] = {e.x, e.y};
-#pragma unroll
-          for (int z = 0; z < 4; ++z) {
-            const uint16_t q2 = (uint16_t)(ew[z >> 1] >> ((z & 1) * 16));
-            const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)q2, __NV_E4M3);
-            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&hr));
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(f.x * sc, f.y * sc);
-            o[z] = *reinterpret_cast<const uint32_t*>(&b2);
-          }
-        };
-        constexpr int U = 4;  // independent items per trip: all loads first, then math, then stores
-        int it = lane;
-        for (; it + 32 * (U - 1) < items; it += 32 * U) {
-          uint32_t xo[U], eo[U];
-          int ri[U];
-          uint4 h[U];
-          uint2 e[U];
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            locate(it + 32 * u, xo[u], eo[u], ri[u]);
-            e[u] = *reinterpret_cast<const uint2*>(es + eo[u]);
-            if (FORM == kFormSplit24) h[u] = *reinterpret_cast<const uint4*>(xs + xo[u]);
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            uint32_t o[4];
-            if (FORM == kFormSplit24) {
-              lo_words(h[u], e[u], o);
-              *reinterpret_cast<uint4*>(xs + xo[u] + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
-            } else {
-              fp8_words(e[u], row_scale[cw][ri[u]], o);
-              *reinterpret_cast<uint4*>(xs + xo[u]) = make_uint4(o[0], o[1], o[2], o[3]);
-            }
-          }
+        for (int z = 0; z < 4; ++z) {
+          const uint32_t eword = ew[z >> 1];
+          const uint32_t sel0 = 0x3200u | ((4u + 2u * (z & 1)) << 4);      // ext byte 2z
+          const uint32_t sel1 = 0x3200u | ((4u + 2u * (z & 1) + 1u) << 4); // ext byte 2z+1
+          const uint32_t h0 = __byte_perm(hw[z], 0u, 0x1044);
+          const uint32_t h1 = hw[z] & 0xFFFF0000u;
+          const uint32_t b0 = __byte_perm(h0, eword, sel0);
+          const uint32_t b1 = __byte_perm(h1, eword, sel1);
+          uint32_t l0, l1;
+          asm("{\n\t.reg .b64 a, b, d;\n\t"
+              "mov.b64 a, {%2, %3};\n\t"
+              "mov.b64 b, {%4, %5};\n\t"
+              "sub.rn.f32x2 d, a, b;\n\t"
+              "mov.b64 {%0, %1}, d;\n\t}"
+              : "=r"(l0), "=r"(l1)
+              : "r"(b0), "r"(b1), "r"(h0), "r"(h1));
+          o[z] = __byte_perm(l0, l1, 0x7632);
         }
-        for (; it < items; it += 32) {
-          uint32_t xo, eo;
-          int ri;
-          locate(it, xo, eo, ri);
-          const uint2 e = *reinterpret_cast<const uint2*>(es + eo);
+      };
+      auto fp8_words = [&](const uint2& e, float sc, uint32_t (&o)[4]) {
+        const uint32_t ew[2] = {e.x, e.y};
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+          const uint16_t q2 = (uint16_t)(ew[z >> 1] >> ((z & 1) * 16));
+          const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)q2, __NV_E4M3);
+          const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&hr));
+          const __nv_bfloat162 b2 = __floats2bfloat162_rn(f.x * sc, f.y * sc);
+          o[z] = *reinterpret_cast<const uint32_t*>(&b2);
+        }
+      };
+      constexpr int U = 4;  // independent items per trip: all loads first, then math, then stores
+      int it = lane;
+      for (; it + 32 * (U - 1) < items; it += 32 * U) {
+        uint32_t xo[U], eo[U];
+        int ri[U];
+        uint4 h[U];
+        uint2 e[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          locate(it + 32 * u, xo[u], eo[u], ri[u]);
+          e[u] = *reinterpret_cast<const uint2*>(es + eo[u]);
+          if (FORM == kFormSplit24) h[u] = *reinterpret_cast<const uint4*>(xs + xo[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
           uint32_t o[4];
           if (FORM == kFormSplit24) {
-            lo_words(*reinterpret_cast<const uint4*>(xs + xo), e, o);
-            *reinterpret_cast<uint4*>(xs + xo + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
+            lo_words(h[u], e[u], o);
+            *reinterpret_cast<uint4*>(xs + xo[u] + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
           } else {
-            fp8_words(e, row_scale[cw][ri], o);
-            *reinterpret_cast<uint4*>(xs + xo) = make_uint4(o[0], o[1], o[2], o[3]);
+            fp8_words(e[u], row_scale[cw][ri[u]], o);
+            *reinterpret_cast<uint4*>(xs + xo[u]) = make_uint4(o[0], o[1], o[2], o[3]);
           }
         }
-        fence_proxy_async_smem();
       }
+      for (; it < items; it += 32) {
+        uint32_t xo, eo;
+        int ri;
+        locate(it, xo, eo, ri);
+        const uint2 e = *reinterpret_cast<const uint2*>(es + eo);
+        uint32_t o[4];
+        if (FORM == kFormSplit24) {
+          lo_words(*reinterpret_cast<const uint4*>(xs + xo), e, o);
+          *reinterpret_cast<uint4*>(xs + xo + 2048) = make_uint4(o[0], o[1], o[2], o[3]);
+        } else {
+          fp8_words(e, row_scale[cw][ri], o);
+          *reinterpret_cast<uint4*>(xs + xo) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+      }
+      fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&full[s]);
-      scv = scn;
+      nb_c = nb_n;
+      sc_c = sc_n;
+      if (nb_c == -2) meta_of(st + kConvWarps, nb_c, sc_c, true);  // not ready when probed
     }
   } else if (warp >= kMmaWarp && warp < kMmaWarp + kMmaWarps) {
     // ------------------------------------------------------------- UMMA
     if (lane == 0) {
       const int m = warp - kMmaWarp;
-      int32_t ws, we;
-      cta_windows(p, c, b0, b1, ws, we);
       constexpr uint32_t idesc = umma_idesc(1, 128, 2 * WH, 1, 0);
       const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 2048, 2);
       const uint64_t bdesc0 = umma_desc(smem_u32(yring), 128, 256, 0);
       uint32_t q = 0;
       bool ok = true;
-      int64_t r0 = ws < we ? __ldg(p.rwo + ws) : 0;
-      int64_t r1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
-      for (int32_t w = ws; w < we && ok; ++w) {
-        const int64_t r2 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;
-        const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
-        r0 = r1;
-        r1 = r2;
-        if (s0 >= s1) continue;
+      for (uint32_t rq = 0; ok; ++rq) {
+        const int rs = (int)(rq % kRecDepth);
+        if (!mbar_wait(&rings.rec_full[rs], (rq / kRecDepth) & 1, p.err)) { ok = false; break; }
+        const WinRec rec = rings.rec[rs];
+        mbar_arrive(&rings.rec_empty[rs]);
+        if (rec.flags & kRecEnd) break;
+        if (rec.flags & kRecEmpty) continue;
+        if (rec.flags & kRecPad) {  // a stage without blocks: its owner passes it on
+          if ((int)(rec.stage_base & 1) == m) {
+            const int s = (int)(rec.stage_base % S);
+            if (!mbar_wait(&full[s], (uint32_t)(rec.stage_base / S) & 1, p.err)) { ok = false; break; }
+            mbar_arrive(&empty[s]);
+          }
+          continue;
+        }
         const int a = (int)(q % K::kNacc);
         if (!mbar_wait(&acc_empty[a], ((q / K::kNacc) & 1) ^ 1, p.err)) { ok = false; break; }
         tc_fence_after();
         const uint32_t dtm = tmem_base + (uint32_t)((m * K::kNacc + a) * K::kAccCols);
         uint32_t acc = 0;
-        int64_t st = (s0 - b0) / P;
-        st += (m - (int)(st % kMmaWarps) + kMmaWarps) % kMmaWarps;
-        const int64_t st_last = (s1 - 1 - b0) / P;
-        for (; st <= st_last; st += kMmaWarps) {
-          const int s = (int)(st % S);
-          const int64_t sb = b0 + st * P;
-          const int64_t lo = sb > s0 ? sb : s0;
-          const int64_t hi = (sb + P) < s1 ? (sb + P) : s1;
-          if (lo == sb) {
-            if (!mbar_wait(&full[s], (uint32_t)(st / S) & 1, p.err)) { ok = false; break; }
-            fence_proxy_async_smem();
+        // this issuer's stages of the window, in order (stage g belongs to
+        // issuer g % 2; chunks start on even stages, so the chunk-relative
+        // index has the same parity)
+        const int64_t rel_first = (rec.wb0 - rec.cb0) / P;
+        const int64_t rel_last = (rec.wb1 - 1 - rec.cb0) / P;
+        for (int64_t rel = rel_first + ((rel_first & 1) != m); rel <= rel_last; rel += kMmaWarps) {
+          const int64_t gst = rec.stage_base + rel;
+          const int s = (int)(gst % S);
+          const int64_t sb = rec.cb0 + rel * P;           // first block of the stage
+          const int64_t lo = sb > rec.wb0 ? sb : rec.wb0;
+          const int64_t hi = (sb + P) < rec.wb1 ? (sb + P) : rec.wb1;
+          const bool last = (hi == sb + P || hi == rec.cb1);  // stage fully consumed
+          if (lo == sb) {  // first visit of this stage (windows are walked in order)
+            if (!mbar_wait(&full[s], (uint32_t)(gst / S) & 1, p.err)) { ok = false; break; }
+            fence_proxy_async_smem();  // cp.async (generic proxy) data -> UMMA reads
             tc_fence_after();
           }
           uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * K::kYB) >> 4);
-          uint64_t adesc =
-              adesc0 + (uint64_t)((s * K::kStageX + (int)(lo - sb) * NT * kTileBytes) >> 4);
+          uint64_t adesc = adesc0 + (uint64_t)((s * K::kStageX +
+                                                (int)(lo - sb) * NT * K::kSub * kTileBytes) >> 4);
           for (int64_t b = lo; b < hi; ++b) {
 #pragma unroll
-            for (int t = 0; t < NT; ++t)
-              mma_f16(dtm + t * 2 * WH, adesc + (uint64_t)(t * (kTileBytes >> 4)), bdesc, idesc,
-                      acc);
+            for (int h = 0; h < K::kSub; ++h)
+#pragma unroll
+              for (int t = 0; t < NT; ++t)
+                mma_f16(dtm + t * 2 * WH,
+                        adesc + (uint64_t)(((t * K::kSub + h) * kTileBytes) >> 4),
+                        bdesc + (uint64_t)((h * K::kYB8) >> 4), idesc, h == 0 ? acc : 1u);
             acc = 1;
-            adesc += (uint64_t)((NT * kTileBytes) >> 4);
+            adesc += (uint64_t)((NT * K::kSub * kTileBytes) >> 4);
             bdesc += (uint64_t)(K::kYB >> 4);
           }
-          if (hi == sb + P || hi == b1) tc_commit(&empty[s]);
+          if (last) tc_commit(&empty[s]);
         }
         if (!ok) break;
         tc_commit(&acc_full[a]);
         ++q;
       }
       if (!ok) *abort_flag = 1;
+      // every MMA this thread issued has finished before the CTA frees TMEM
+      // (also when a wait gave up with MMAs in flight)
+      tc_commit(&drain[m]);
+      mbar_wait(&drain[m], 0, p.err);
     }
     __syncwarp();
-  } else {
+  } else if (warp < kEpiWarps) {
     // --------------------------------------------------------- epilogue
-    int32_t ws, we;
-    cta_windows(p, c, b0, b1, ws, we);
     const int ew = warp;
     uint32_t q = 0;
     uint32_t su = 0;  // C tiles this warp has staged (selects the staging buffer)
-    int64_t rn0 = ws < we ? __ldg(p.rwo + ws) : 0;
-    int64_t rn1 = ws < we ? __ldg(p.rwo + ws + 1) : 0;
-    for (int32_t w = ws; w < we; ++w) {
-      const int64_t r0 = rn0, r1 = rn1;
-      rn0 = rn1;
-      rn1 = (w + 2 <= p.nwin) ? __ldg(p.rwo + w + 2) : 0;
-      const int64_t row0 = (int64_t)w * WH;
-      if (r0 == r1) {
-        for (int f = col0 + ew * 32 + lane; f < col0 + ncols; f += 128)
-          for (int r = 0; r < WH && row0 + r < p.M; ++r)
-            p.C[(row0 + r) * p.N + f] = epilogue(p, 0.0f, f);
+    for (uint32_t rq = 0;; ++rq) {
+      const int rs = (int)(rq % kRecDepth);
+      if (!warp_wait(&rings.rec_full[rs], (rq / kRecDepth) & 1, p.err, abort_flag)) break;
+      const WinRec rec = rings.rec[rs];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&rings.rec_empty[rs]);
+      if (rec.flags & kRecEnd) break;
+      if (rec.flags & kRecPad) continue;
+      if (rec.flags & kRecEmpty) {
+        zero_window_rows(p, rec.w, col0, ncols, ew * 32 + lane, 32 * kEpiWarps);
         continue;
       }
-      const int64_t s0 = r0 > b0 ? r0 : b0, s1 = r1 < b1 ? r1 : b1;
-      if (s0 >= s1) continue;
       const int a = (int)(q % K::kNacc);
-      const bool got = mbar_wait(&acc_full[a], (q / K::kNacc) & 1, p.err);
-      if (!__all_sync(0xffffffffu, got)) { *abort_flag = 1; break; }
+      if (!warp_wait(&acc_full[a], (q / K::kNacc) & 1, p.err, abort_flag)) break;
       tc_fence_after();
+      const int64_t row0 = (int64_t)rec.w * WH;
       float* out;
       bool guard_rows = true;
-      if (p.mode == 1 && (r0 < b0 || r1 > b1)) {
-        const int slot = (r0 < b0) ? 2 * c : 2 * c + 1;
+      if (p.mode == 1 && (rec.flags & (kRecHead | kRecTail))) {
+        const int slot = (rec.flags & kRecHead) ? 2 * rec.chunk : 2 * rec.chunk + 1;
         out = p.part + (size_t)slot * WH * p.N;
         guard_rows = false;
       } else {
         out = p.C + row0 * p.N;
       }
-      const int64_t st0 = (s0 - b0) / P, st1 = (s1 - 1 - b0) / P;
+      const int64_t st0 = (rec.wb0 - rec.cb0) / P, st1 = (rec.wb1 - 1 - rec.cb0) / P;
       const bool both = st1 > st0;
       const int m0 = (int)(st0 % kMmaWarps);
       const uint32_t lane_addr = tmem_base + ((uint32_t)(ew * 32) << 16);
@@ -609,26 +669,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_split(const __grid_constan
 
   tc_fence_before();
   __syncthreads();
+  if (threadIdx.x == 0 && p.stamps) {
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    record_cta_time(p, 0, t_entry);
+    record_cta_time(p, 1, global_timer_ns());
+    record_cta_time(p, 2, smid);
+  }
   if (warp == kMmaWarp) {
     tc_fence_after();
     tmem_dealloc(tmem_base, K::kTmemCols);
   }
 }
 
-template <int FORM, int NT, int P, int S, bool FOUR, int WH>
+template <int FORM, int NT, int P, int S, bool FOUR, int WH, int BW>
 dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
-  constexpr int smem = SCfg<FORM, NT, P, S, WH>::kSmem;
+  using K = SCfg<FORM, NT, P, S, WH, BW>;
+  constexpr int smem = K::kSmem;
   static_assert(smem <= 227 * 1024, "shared memory budget");
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev & 63]) {
-    DTC_CUDA(cudaFuncSetAttribute(k_spmm_split<FORM, NT, P, S, FOUR, WH>,
+    DTC_CUDA(cudaFuncSetAttribute(k_spmm_split<FORM, NT, P, S, FOUR, WH, BW>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr_set[dev & 63] = true;
   }
-  dim3 grid((unsigned)p.G, (unsigned)slices);
-  k_spmm_split<FORM, NT, P, S, FOUR, WH><<<grid, kThreads, smem, st>>>(p);
+  dim3 grid((unsigned)launch_ctas(p, slices), (unsigned)slices);
+  k_spmm_split<FORM, NT, P, S, FOUR, WH, BW><<<grid, K::kThreads, smem, st>>>(p);
   DTC_CUDA(cudaGetLastError());
   if (p.mode == 1 && p.G > 1) {
     k_reduce_partials<<<p.G - 1, 256, 0, st>>>(p);
@@ -640,19 +708,21 @@ dtc_status launch_split(const Params& p, int slices, cudaStream_t st) {
 // N-tiles per CTA: all of N up to 4 (window height 16) or 2 (height 32, whose
 // accumulators are twice as wide) unless capped by `ntile`.
 template <int FORM, bool FOUR>
-dtc_status dispatch_n(const Params& p, cudaStream_t st, int ntile) {
-  int nt = p.N <= 128 ? 1 : p.N <= 256 ? 2 : 4;
-  if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
+dtc_status dispatch_n(const Params& p, int nt, int W, int slices, cudaStream_t st) {
+  if (W == 16) {  // 16 gathered rows per block: half the blocks per stage
+    if (nt == 1) return launch_split<FORM, 1, 2, 8, FOUR, 16, 16>(p, slices, st);
+    return launch_split<FORM, 2, 1, 8, FOUR, 16, 16>(p, slices, st);
+  }
   if (p.H == 32) {
     // forms with a staging ring for the second plane hold 3 blocks per stage so
     // the 32-row A tiles fit in shared memory; the others keep 4
     constexpr int P32 = (FORM == kFormBF16 || FORM == kFormBF16X2) ? 4 : 3;
-    if (nt == 1) return launch_split<FORM, 1, P32, 8, FOUR, 32>(p, (p.N + 127) / 128, st);
-    return launch_split<FORM, 2, 2, 8, FOUR, 32>(p, (p.N + 255) / 256, st);
+    if (nt == 1) return launch_split<FORM, 1, P32, 8, FOUR, 32, 8>(p, slices, st);
+    return launch_split<FORM, 2, 2, 8, FOUR, 32, 8>(p, slices, st);
   }
-  if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 16>(p, (p.N + 127) / 128, st);
-  if (nt == 2) return launch_split<FORM, 2, 2, 8, FOUR, 16>(p, (p.N + 255) / 256, st);
-  return launch_split<FORM, 4, 1, 8, FOUR, 16>(p, (p.N + 511) / 512, st);
+  if (nt == 1) return launch_split<FORM, 1, 4, 8, FOUR, 16, 8>(p, slices, st);
+  if (nt == 2) return launch_split<FORM, 2, 2, 8, FOUR, 16, 8>(p, slices, st);
+  return launch_split<FORM, 4, 1, 8, FOUR, 16, 8>(p, slices, st);
 }
 
 }  // namespace
@@ -661,7 +731,8 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            const int32_t* s2x, const float* vals, int32_t M, int32_t nwin,
                            int64_t T, int bformat, const void* p0, const void* p1, int32_t N,
                            int precision, float* C, int mode, int grid, float* part,
-                           cudaStream_t st, int ntile, Epilogue epi, int H) {
+                           cudaStream_t st, int ntile, Epilogue epi, int H, void* queue,
+                           int W) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
   DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8 ||
                   bformat == DTC_B_BF16X2,
@@ -671,7 +742,10 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   DTC_REQUIRE(N % 16 == 0, "split forms need N % 16 == 0 (16-byte row segments of every plane)");
   DTC_REQUIRE(bformat == DTC_B_BF16 || p1 != nullptr, "second B plane missing");
   DTC_REQUIRE(((uintptr_t)p0 & 15) == 0 && ((uintptr_t)p1 & 15) == 0, "planes must be 16-byte aligned");
+  DTC_REQUIRE(((uintptr_t)s2x & 15) == 0, "SparseAToX must be 16-byte aligned");
   DTC_REQUIRE(H == 16 || H == 32, "window height must be 16 or 32");
+  DTC_REQUIRE(W == 8 || (W == 16 && H == 16),
+              "block width must be 8, or 16 at window height 16 (tile ids are bytes)");
   DTC_REQUIRE(nwin == (M + H - 1) / H, "num_windows must be ceil(num_nodes / window height)");
   DTC_REQUIRE(mode == 0 || part != nullptr, "balance mode needs the partials workspace");
   if (!is_sm100()) {
@@ -692,23 +766,29 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
   DTC_REQUIRE(((uintptr_t)C & 15) == 0, "C must be 16-byte aligned");
   dtc_status es = encode_c_map(&p.cmap, C, M, N, 16);
   if (es != DTC_OK) return es;
-  int G = grid > 0 ? grid : default_grid();
+  int G = grid > 0 ? grid : default_chunks();
   if ((int64_t)G > T) G = (int)T;
   p.G = G;
+  int nt = N <= 128 ? 1 : N <= 256 ? 2 : 4;
+  if (ntile == 1 || ntile == 2) nt = nt < ntile ? nt : ntile;
+  if ((H == 32 || W == 16) && nt > 2) nt = 2;
+  const int slices = (N + nt * 128 - 1) / (nt * 128);
+  es = setup_queue(p, queue, slices, st);
+  if (es != DTC_OK) return es;
   const bool four = precision == DTC_PREC_SPLIT4;
   switch (bformat) {
     case DTC_B_SPLIT24:
-      return four ? dispatch_n<kFormSplit24, true>(p, st, ntile)
-                  : dispatch_n<kFormSplit24, false>(p, st, ntile);
+      return four ? dispatch_n<kFormSplit24, true>(p, nt, W, slices, st)
+                  : dispatch_n<kFormSplit24, false>(p, nt, W, slices, st);
     case DTC_B_BF16:
-      return four ? dispatch_n<kFormBF16, true>(p, st, ntile)
-                  : dispatch_n<kFormBF16, false>(p, st, ntile);
+      return four ? dispatch_n<kFormBF16, true>(p, nt, W, slices, st)
+                  : dispatch_n<kFormBF16, false>(p, nt, W, slices, st);
     case DTC_B_BF16X2:
-      return four ? dispatch_n<kFormBF16X2, true>(p, st, ntile)
-                  : dispatch_n<kFormBF16X2, false>(p, st, ntile);
+      return four ? dispatch_n<kFormBF16X2, true>(p, nt, W, slices, st)
+                  : dispatch_n<kFormBF16X2, false>(p, nt, W, slices, st);
     default:
-      return four ? dispatch_n<kFormFP8, true>(p, st, ntile)
-                  : dispatch_n<kFormFP8, false>(p, st, ntile);
+      return four ? dispatch_n<kFormFP8, true>(p, nt, W, slices, st)
+                  : dispatch_n<kFormFP8, false>(p, nt, W, slices, st);
   }
 }
 

@@ -13,14 +13,18 @@
 //      (band, band-hash) keys). Each item is paired with the next
 //      `bucket_window` items of its bucket (the reference pairs every bucket
 //      member; the window bounds hub buckets).
-//   3. Exact Jaccard similarity of every distinct candidate pair (host).
+//   3. Exact Jaccard similarity of every distinct candidate pair (GPU, one
+//      thread per pair merging the two sorted sets), then a stable radix sort
+//      of the pairs by descending similarity (ties keep the (first, second)
+//      order of the sorted pair list).
 //   4. Greedy merging by descending similarity with union-find, exactly the
 //      reference's loop (:171-205 / :268-293): two live roots merge (smaller
 //      size into larger; ties into the first of the pair); a cluster whose
 //      size reaches the cap (`thres` rows at level 1, `c_thres` clusters at
 //      level 2) stops merging; a pair whose ends are no longer roots is
 //      requeued once as (root, root) with the Jaccard of the two roots' own
-//      item sets. Ties in similarity pop in (first, second) order.
+//      item sets. Ties in similarity pop in (first, second) order. The loop
+//      walks the sorted initial pairs and keeps only requeued pairs in a heap.
 // Clusters are numbered in order of their smallest member, members ascending;
 // the output lists level-2 groups in that order, each group's clusters in
 // ascending number and each cluster's rows ascending (:308-315).
@@ -132,11 +136,54 @@ __global__ void k_bucket_pairs(const uint64_t* __restrict__ keys, const int32_t*
   }
 }
 
+// score[i] = Jaccard of the sorted, distinct sets of the two items of pair i
+// (hi << 32 | lo packing: lo < hi), exactly (double)|a ∩ b| / |a ∪ b| as the
+// host computes it; 0 when either set is empty.
+__global__ void k_pair_jaccard(const uint64_t* __restrict__ pairs, int64_t np,
+                               const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                               double* __restrict__ score) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += stride) {
+    const uint64_t pr = pairs[i];
+    const int32_t a = (int32_t)(pr >> 32), b = (int32_t)(pr & 0xffffffffu);
+    int64_t ia = ptr[a], ea = ptr[a + 1], ib = ptr[b], eb = ptr[b + 1];
+    const int64_t na = ea - ia, nb = eb - ib;
+    double s = 0.0;
+    if (na > 0 && nb > 0) {
+      int64_t inter = 0;
+      int32_t va = idx[ia], vb = idx[ib];
+      while (true) {
+        if (va < vb) {
+          if (++ia == ea) break;
+          va = idx[ia];
+        } else if (va > vb) {
+          if (++ib == eb) break;
+          vb = idx[ib];
+        } else {
+          ++inter;
+          if (++ia == ea || ++ib == eb) break;
+          va = idx[ia];
+          vb = idx[ib];
+        }
+      }
+      s = (double)inter / (double)(na + nb - inter);
+    }
+    score[i] = s;
+  }
+}
+
 // Device workspace for one level over n items with P-value signatures.
 struct LshLayout {
   size_t keys_in, keys_out, items_in, items_out, counts, offs, pairs_in, pairs_out, sort1, scan,
-      sort2, total;
+      sort2, uniq, nsel, score_in, score_out, ord_in, ord_out, sort3, total;
 };
+
+// ord[i] = i.
+__global__ void k_iota(int32_t* __restrict__ ord, int64_t n) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    ord[i] = (int32_t)i;
+}
 
 LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
   LshLayout L{};
@@ -152,23 +199,46 @@ LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
   L.offs = take((n + 1) * 4);
   L.pairs_in = take(mp * 8);
   L.pairs_out = take(mp * 8);
-  size_t s1 = 0, s2 = 0, s3 = 0;
+  size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, s1, (uint64_t*)nullptr, (uint64_t*)nullptr,
                                   (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n);
   cub::DeviceScan::ExclusiveSum(nullptr, s2, (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n + 1);
   cub::DeviceRadixSort::SortKeys(nullptr, s3, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)mp);
+  cub::DeviceSelect::Unique(nullptr, s5, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                            (int64_t*)nullptr, (int64_t)mp);
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, s4, (double*)nullptr, (double*)nullptr,
+                                            (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)mp);
   L.sort1 = take(s1);
   L.scan = take(s2);
   L.sort2 = take(s3);
+  L.uniq = take(s5);
+  L.nsel = take(8);
+  L.score_in = take(mp * 8);
+  L.score_out = take(mp * 8);
+  L.ord_in = take(mp * 4);
+  L.ord_out = take(mp * 4);
+  L.sort3 = take(s4);
   L.total = off;
   return L;
 }
 
-// Candidate pairs (lo, hi), lo < hi, sorted and distinct, for n items.
+// Candidate pairs of one level: distinct (lo << 32 | hi, lo < hi) in ascending
+// order, their Jaccard scores, and the order of descending score (ties in
+// ascending pair order).
+struct Scored {
+  std::vector<uint64_t> keys;
+  std::vector<int32_t> order;   // indices into keys, best first
+  std::vector<double> score;    // score of keys[order[j]]
+};
+
+// Candidate pairs for n items whose sorted, distinct sets are d_ptr / d_idx
+// (device CSR), scored on the GPU.
 dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, char* ws,
-                     const LshLayout& L, int64_t max_pairs, cudaStream_t st,
-                     std::vector<uint64_t>& out) {
-  out.clear();
+                     const LshLayout& L, int64_t max_pairs, const int64_t* d_ptr,
+                     const int32_t* d_idx, cudaStream_t st, Scored& out) {
+  out.keys.clear();
+  out.order.clear();
+  out.score.clear();
   if (n < 2) return DTC_OK;
   const int64_t nk = (int64_t)n * prm.bands;
   uint64_t* kin = (uint64_t*)(ws + L.keys_in);
@@ -198,14 +268,31 @@ dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, 
   }
   k_bucket_pairs<<<grid_for(nk), kThreads, 0, st>>>(kout, iout, nk, prm.bucket_window, counts,
                                                     offs, pin);
-  size_t b3 = L.total - L.sort2;
+  size_t b3 = L.uniq - L.sort2;
   DTC_CUDA(cub::DeviceRadixSort::SortKeys(ws + L.sort2, b3, pin, pout, (int64_t)np, 0, 64, st));
-  std::vector<uint64_t> h(np);
-  DTC_CUDA(cudaMemcpyAsync(h.data(), pout, (size_t)np * 8, cudaMemcpyDeviceToHost, st));
+  int64_t* nsel = (int64_t*)(ws + L.nsel);
+  size_t b4 = L.nsel - L.uniq;
+  DTC_CUDA(cub::DeviceSelect::Unique(ws + L.uniq, b4, pout, pin, nsel, (int64_t)np, st));
+  int64_t nu = 0;
+  DTC_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
   DTC_CUDA(cudaStreamSynchronize(st));
-  out.reserve(np);
-  for (int32_t i = 0; i < np; ++i)
-    if (i == 0 || h[i] != h[i - 1]) out.push_back(h[i]);
+  double* sin = (double*)(ws + L.score_in);
+  double* sout = (double*)(ws + L.score_out);
+  int32_t* oin = (int32_t*)(ws + L.ord_in);
+  int32_t* oout = (int32_t*)(ws + L.ord_out);
+  k_pair_jaccard<<<grid_for(nu), kThreads, 0, st>>>(pin, nu, d_ptr, d_idx, sin);
+  k_iota<<<grid_for(nu), kThreads, 0, st>>>(oin, nu);
+  DTC_CUDA(cudaGetLastError());
+  size_t b5 = L.total - L.sort3;
+  DTC_CUDA(cub::DeviceRadixSort::SortPairsDescending(ws + L.sort3, b5, sin, sout, oin, oout, nu,
+                                                     0, 64, st));
+  out.keys.resize(nu);
+  out.order.resize(nu);
+  out.score.resize(nu);
+  DTC_CUDA(cudaMemcpyAsync(out.keys.data(), pin, (size_t)nu * 8, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaMemcpyAsync(out.order.data(), oout, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaMemcpyAsync(out.score.data(), sout, (size_t)nu * 8, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaStreamSynchronize(st));
   return DTC_OK;
 }
 
@@ -241,9 +328,10 @@ struct QItem {
   }
 };
 
-// The greedy merge loop; returns the root of every item.
-std::vector<int32_t> greedy_merge(const Sets& sets, const std::vector<uint64_t>& pairs,
-                                  int32_t n, int32_t cap) {
+// The greedy merge loop; returns the root of every item. The initial pairs
+// come sorted (Scored); requeued (root, root) pairs go to a heap, and the next
+// pair is the better of the two heads in the QItem order.
+std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n, int32_t cap) {
   std::vector<int32_t> parent(n), size(n, 1);
   std::vector<char> deleted(n, 0);
   for (int32_t i = 0; i < n; ++i) parent[i] = i;
@@ -254,23 +342,43 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const std::vector<uint64_t>&
     }
     return i;
   };
-  std::priority_queue<QItem> q;
-  std::unordered_set<uint64_t> inset;  // pairs currently queued (lo << 32 | hi)
-  inset.reserve(pairs.size() * 2 + 16);
   auto key = [](int32_t a, int32_t b) {
     return a < b ? ((uint64_t)a << 32) | (uint32_t)b : ((uint64_t)b << 32) | (uint32_t)a;
   };
-  for (uint64_t p : pairs) {
-    const int32_t a = (int32_t)(p >> 32), b = (int32_t)(p & 0xffffffffu);
-    q.push({sets.jac(a, b), a, b});
-    inset.insert(p);
-  }
+  const int64_t np = (int64_t)sp.keys.size();
+  std::vector<int32_t> rank(np);  // position of keys[t] in the sorted order
+  for (int64_t j = 0; j < np; ++j) rank[sp.order[j]] = (int32_t)j;
+  int64_t next = 0;  // initial pairs before `next` have been popped
+  std::priority_queue<QItem> q;
+  std::unordered_set<uint64_t> requeued;  // pairs currently in the heap
+  // a pair is queued when it is an initial pair not popped yet, or in the heap
+  auto queued = [&](uint64_t k) {
+    const auto it = std::lower_bound(sp.keys.begin(), sp.keys.end(), k);
+    if (it != sp.keys.end() && *it == k && rank[it - sp.keys.begin()] >= next) return true;
+    return requeued.count(k) > 0;
+  };
   int64_t num_cluster = n;
-  while (!q.empty() && num_cluster > 0) {
-    const QItem it = q.top();
-    q.pop();
+  while (num_cluster > 0) {
+    QItem it;
+    bool from_init;
+    if (next < np) {
+      const uint64_t k0 = sp.keys[sp.order[next]];
+      const QItem a{sp.score[next], (int32_t)(k0 >> 32), (int32_t)(k0 & 0xffffffffu)};
+      from_init = q.empty() || !(a < q.top());
+      it = from_init ? a : q.top();
+    } else if (!q.empty()) {
+      from_init = false;
+      it = q.top();
+    } else {
+      break;
+    }
+    if (from_init) {
+      ++next;
+    } else {
+      q.pop();
+      requeued.erase(key(it.a, it.b));
+    }
     int32_t p1 = it.a, p2 = it.b;
-    inset.erase(key(p1, p2));
     if (p1 == parent[p1] && p2 == parent[p2]) {
       if (deleted[p1] || deleted[p2]) continue;
       if (size[p1] < size[p2]) {
@@ -288,9 +396,9 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const std::vector<uint64_t>&
       p1 = root(p1);
       p2 = root(p2);
       if (deleted[p1] || deleted[p2]) continue;
-      if (p1 != p2 && !inset.count(key(p1, p2))) {
+      if (p1 != p2 && !queued(key(p1, p2))) {
         q.push({sets.jac(p1, p2), p1, p2});
-        inset.insert(key(p1, p2));
+        requeued.insert(key(p1, p2));
       }
     }
   }
@@ -351,6 +459,8 @@ dtc_status dtc_tca_workspace_bytes(int32_t num_nodes, int64_t nnz, const dtc_tca
   const LshLayout L = lsh_layout(nk, nk * p.bucket_window);
   size_t off = align_up((size_t)n * p.num_perm * 4, 256) * 2;  // row + cluster signatures
   off += align_up((size_t)n * 4, 256);                          // cluster id per row
+  off += align_up((size_t)(n + 1) * 8, 256);                    // item sets: offsets
+  off += align_up((size_t)(nnz > 0 ? nnz : 1) * 4, 256);        //            members
   *bytes = off + L.total;
   return DTC_OK;
 }
@@ -392,15 +502,24 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
       set_error("tca: rowptr must be non-decreasing");
       return DTC_ERR_INVALID_ARGUMENT;
     }
-    std::vector<int32_t> v(hcol.begin() + hrp[r], hcol.begin() + hrp[r + 1]);
-    std::sort(v.begin(), v.end());
-    v.erase(std::unique(v.begin(), v.end()), v.end());
-    for (int32_t c : v)
-      if (c < 0 || c >= M) {
+    const int32_t* b = hcol.data() + hrp[r];
+    const int32_t* e = hcol.data() + hrp[r + 1];
+    bool canon = true;  // sorted and distinct already (canonical CSR): no copy to sort
+    for (const int32_t* x = b; x < e; ++x) {
+      if (*x < 0 || *x >= M) {
         set_error("tca: column index out of range");
         return DTC_ERR_INVALID_ARGUMENT;
       }
-    rows.idx.insert(rows.idx.end(), v.begin(), v.end());
+      if (x > b && x[-1] >= *x) canon = false;
+    }
+    if (canon) {
+      rows.idx.insert(rows.idx.end(), b, e);
+    } else {
+      std::vector<int32_t> v(b, e);
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      rows.idx.insert(rows.idx.end(), v.begin(), v.end());
+    }
     rows.ptr[r + 1] = (int64_t)rows.idx.size();
   }
   char* ws = (char*)d_workspace;
@@ -408,7 +527,16 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
   uint32_t* rsig = (uint32_t*)ws;
   uint32_t* csig = (uint32_t*)(ws + sig_bytes);
   int32_t* cid = (int32_t*)(ws + 2 * sig_bytes);
-  char* lws = ws + 2 * sig_bytes + align_up((size_t)M * 4, 256);
+  int64_t* d_set_ptr = (int64_t*)(ws + 2 * sig_bytes + align_up((size_t)M * 4, 256));
+  int32_t* d_set_idx = (int32_t*)((char*)d_set_ptr + align_up((size_t)(M + 1) * 8, 256));
+  char* lws = (char*)d_set_idx + align_up((size_t)(nnz > 0 ? nnz : 1) * 4, 256);
+  auto upload = [&](const Sets& x) -> dtc_status {
+    DTC_CUDA(cudaMemcpyAsync(d_set_ptr, x.ptr.data(), x.ptr.size() * 8, cudaMemcpyHostToDevice, st));
+    if (!x.idx.empty())
+      DTC_CUDA(cudaMemcpyAsync(d_set_idx, x.idx.data(), x.idx.size() * 4, cudaMemcpyHostToDevice,
+                               st));
+    return DTC_OK;
+  };
   const int64_t nk = (int64_t)M * p.bands;
   const int64_t max_pairs = nk * p.bucket_window;
   const LshLayout L = lsh_layout(nk, max_pairs);
@@ -417,8 +545,10 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
   k_row_signatures<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(d_rowptr, d_col, M, p.num_perm,
                                                                    p.seed, rsig);
   DTC_CUDA(cudaGetLastError());
-  std::vector<uint64_t> pairs;
-  s = lsh_pairs(rsig, M, p, lws, L, max_pairs, st, pairs);
+  Scored pairs;
+  s = upload(rows);
+  if (s != DTC_OK) return s;
+  s = lsh_pairs(rsig, M, p, lws, L, max_pairs, d_set_ptr, d_set_idx, st, pairs);
   if (s != DTC_OK) return s;
   const auto groups1 = groups_of(greedy_merge(rows, pairs, M, p.thres));
   const int32_t nc = (int32_t)groups1.size();
@@ -444,7 +574,9 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
   k_cluster_signatures<<<grid_for((int64_t)M * p.num_perm), kThreads, 0, st>>>(rsig, cid, M,
                                                                               p.num_perm, csig);
   DTC_CUDA(cudaGetLastError());
-  s = lsh_pairs(csig, nc, p, lws, L, max_pairs, st, pairs);
+  s = upload(cl);
+  if (s != DTC_OK) return s;
+  s = lsh_pairs(csig, nc, p, lws, L, max_pairs, d_set_ptr, d_set_idx, st, pairs);
   if (s != DTC_OK) return s;
   const auto groups2 = groups_of(greedy_merge(cl, pairs, nc, p.c_thres));
 

@@ -81,14 +81,16 @@ dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, i
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
   DTC_REQUIRE(block_h == 16 || block_h == 32, "block_h must be 16 or 32");
-  *bytes = spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms(), block_h);
+  *bytes = align_up(spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms(), block_h), 256) +
+           spmm_queue_bytes(num_blocks, kMaxWaves * num_sms());
   return DTC_OK;
 }
 
 dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                         const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                         const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                        int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
+                        int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                        const void* d_Bplane0,
                         const void* d_Bplane1, int32_t N, int precision, float* d_C,
                         void* d_workspace, size_t workspace_bytes, int reps,
                         dtc_schedule* results, int max_results, int* num_results, int* best,
@@ -118,6 +120,11 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
   DTC_CUDA(cudaEventCreate(&ev.a));
   DTC_CUDA(cudaEventCreate(&ev.b));
   const int sms = num_sms();
+  // the chunk queue sits after the largest candidate's partial tiles
+  void* queue = queue_region(
+      d_workspace, workspace_bytes,
+      align_up(spmm_partials_bytes(num_blocks, N, kMaxWaves * sms, block_h), 256), num_blocks,
+      kMaxWaves * sms);
   int best_i = -1;
   for (int i = 0; i < ncand; ++i) {
     dtc_schedule& c = cand[i];
@@ -128,11 +135,13 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
       return tf32 ? spmm_tf32_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
                                    d_tcValues, num_nodes, num_windows, num_blocks,
                                    (const float*)d_Bplane0, N, d_C, c.mode, c.grid,
-                                   (float*)d_workspace, st, c.ntile, Epilogue{}, block_h)
+                                   (float*)d_workspace, st, c.ntile, Epilogue{}, block_h, queue,
+                                   block_w)
                   : spmm_split_impl(d_rowWindowOffset, d_tileId, d_tcblockOffset, d_sparseAToX,
                                     d_tcValues, num_nodes, num_windows, num_blocks, bformat,
                                     d_Bplane0, d_Bplane1, N, precision, d_C, c.mode, c.grid,
-                                    (float*)d_workspace, st, c.ntile, Epilogue{}, block_h);
+                                    (float*)d_workspace, st, c.ntile, Epilogue{}, block_h, queue,
+                                    block_w);
     };
     s = run();  // warm-up
     if (s != DTC_OK) return s;

@@ -33,12 +33,13 @@ SIGNATURES = {
     "dtc_spmm": [vp, vp, vp, vp, vp, i32, i32, i64, vp, i32, vp, vp],
     "dtc_spmm_balance_workspace_bytes": [i32, i64, i32, szp],
     "dtc_spmm_balance": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp, sz, vp],
-    "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp,
-                    C.c_int, C.c_int, C.c_int, vp, sz, vp],
+    "dtc_spmm_ex": [vp, vp, vp, vp, vp, i32, i32, i64, i32, i32, C.c_int, vp, vp, i32, C.c_int,
+                    vp, C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_spmm_ex_workspace_bytes": [i32, i64, i32, i32, C.c_int, C.c_int, szp],
-    "dtc_spmm_fused": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp,
-                       C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, sz, vp],
+    "dtc_spmm_fused": [vp, vp, vp, vp, vp, i32, i32, i64, i32, i32, C.c_int, vp, vp, i32,
+                       C.c_int, vp, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, sz, vp],
     "dtc_rowid_to_window_offset": [vp, i64, i32, vp, vp],
+    "dtc_set_cta_timer": [vp, i32],
     "dtc_spmm_mma_sync": [vp, vp, vp, vp, vp, i32, i32, vp, i32, vp, vp],
     "dtc_spmm_balance_noalloc": [vp, vp, vp, vp, vp, i32, i64, vp, i32, vp, vp],
     "dtc_noalloc_scratch_capacity": [],
@@ -60,8 +61,8 @@ SIGNATURES = {
     "dtc_transpose_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_coo_to_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_autotune_workspace_bytes": [i32, i64, i32, i32, szp],
-    "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, i32, C.c_int, vp, vp, i32, C.c_int, vp, vp, sz,
-                     C.c_int, vp, C.c_int, vp, vp, vp],
+    "dtc_autotune": [vp, vp, vp, vp, vp, i32, i32, i64, i32, i32, C.c_int, vp, vp, i32, C.c_int,
+                     vp, vp, sz, C.c_int, vp, C.c_int, vp, vp, vp],
 }
 _RESTYPES = {"dtc_last_error": C.c_char_p, "dtc_version": C.c_int,
              "dtc_noalloc_scratch_capacity": C.c_size_t, "dtc_schedule_candidates": C.c_int,

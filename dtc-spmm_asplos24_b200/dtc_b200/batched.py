@@ -3,12 +3,14 @@
 The matrices are stacked block-diagonally with each matrix's rows padded to a
 whole number of 16-row windows, so no row window mixes two matrices and the
 ME-TCF of the stack is exactly the union of the per-matrix ME-TCFs. One
-conversion covers the whole batch, and one launch of the persistent
-strict-balance kernel multiplies every matrix with its own dense operand:
-the CTAs split the batch's TC blocks into equal contiguous ranges, which is the
-global row-window work queue (a CTA that drains its range early is replaced by
-the next wave). The launch (plus its partial-tile reduction) can be captured in
-a CUDA graph and replayed.
+conversion covers the whole batch, and one launch multiplies every matrix
+with its own dense operand: the batch's TC blocks are cut into chunks
+(contiguous block ranges, snapped to row windows in window mode) and one CTA
+per SM pulls chunk ids from a device counter, the global work queue, until
+the batch is done (queue=False runs one CTA per chunk instead, handed out by
+the hardware block scheduler). The launch (plus its small chunk-table kernel
+and, in balance mode, its partial-tile reduction) can be captured in a CUDA
+graph and replayed.
 
 There is no counterpart in the reference, which multiplies one matrix per
 call (DTC-SpMM/DTCSpMM.cpp:117-178).
@@ -71,7 +73,8 @@ class BatchedSpMM:
     returns per-matrix views.
     """
 
-    def __init__(self, mats, N: int, device="cuda", fmt=None, precision=None, mode=1, grid=0):
+    def __init__(self, mats, N: int, device="cuda", fmt=None, precision=None, mode=1, grid=0,
+                 queue=True):
         from ._lib import B_F32, PREC_TF32
         rowptr, col, val, self.layout = stack_csr(mats)
         self.N = N
@@ -84,9 +87,17 @@ class BatchedSpMM:
         self.B = torch.zeros((self.layout.total_rows, N), dtype=torch.float32, device=self.device)
         self.C = torch.empty((self.layout.total_rows, N), dtype=torch.float32, device=self.device)
         self.planes = None
-        self.ws = torch.empty(max(_m.spmm_balance_workspace_bytes(self.m, N), 1),
-                              dtype=torch.uint8, device=self.device)
+        self.queue = queue
+        self._alloc_ws()
         self.graph: Optional[torch.cuda.CUDAGraph] = None
+
+    def _alloc_ws(self):
+        """Workspace of the current schedule: partial tiles (balance mode) and,
+        with queue=True, the chunk-queue region after them."""
+        full = _m.spmm_ex_workspace_bytes(self.m, self.N, self.mode, self.grid)
+        q = _m.spmm_ex_workspace_bytes(self.m, self.N, 0, self.grid)
+        wsb = full if self.queue else full - q
+        self.ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=self.device)
 
     def autotune(self, heights=(16, 32), reps=3):
         """Exhaustive schedule search for this batch (dtc_autotune): window height
@@ -109,8 +120,7 @@ class BatchedSpMM:
                 best = (mm, b)
         self.m, sched = best
         self.mode, self.grid, self.ntile = sched.mode, sched.grid, sched.ntile
-        self.ws = torch.empty(max(tune.workspace_for(self.m, self.N, self.device).numel(), 1),
-                              dtype=torch.uint8, device=self.device)
+        self._alloc_ws()
         self.graph = None
         return table
 
@@ -171,6 +181,23 @@ def separate_launches(mats, N, device="cuda"):
             _m.spmm(mm, b, out=o)
         return outs
     return ms, run
+
+
+def separate_launches_graph(ms, Bs, outs, device="cuda"):
+    """The per-matrix launches of separate_launches captured in ONE CUDA graph:
+    the kernel-level baseline for the single batched launch (no host launch
+    overhead between the matrices). Returns the graph; replay() reruns them."""
+    s = torch.cuda.Stream(device)
+    s.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(s):
+        for mm, b, o in zip(ms, Bs, outs):
+            _m.spmm(mm, b, out=o)
+    torch.cuda.current_stream(device).wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for mm, b, o in zip(ms, Bs, outs):
+            _m.spmm(mm, b, out=o)
+    return g
 
 
 def zipf_batch(count=512, N=64, seed=0, rows_lo=256, rows_hi=65536, s=2.1, dmin=1, dmax=2000):

@@ -149,26 +149,31 @@ def pack_b_into(B: torch.Tensor, fmt: int, planes):
 
 
 def spmm_ex_workspace_bytes(m: METCF, N, mode=0, grid=0):
-    """Workspace bytes spmm_ex needs for this schedule (0 in window mode)."""
+    """Workspace bytes of spmm_ex for this schedule: the partial tiles of balance
+    mode (required) and the chunk-queue region after them (optional: without it
+    the kernels run one CTA per chunk instead of persistent CTAs)."""
     wsb = C.c_size_t()
     call("dtc_spmm_ex_workspace_bytes", m.M, m.T, N, m.H, mode, grid, C.byref(wsb))
     return wsb.value
 
 
-def spmm_ex_launches(m: METCF, mode=0, grid=0):
-    """Kernels one spmm_ex call launches: the SpMM, plus the partial-tile
-    reduction in balance mode when more than one CTA shares the blocks."""
+def spmm_ex_launches(m: METCF, mode=0, grid=0, queue=True):
+    """Kernels one spmm_ex call launches: the chunk-table kernel (when the
+    workspace holds the chunk queue), the SpMM, and the partial-tile reduction
+    in balance mode when the blocks are cut into more than one chunk."""
     if m.T == 0:
         return 0
     sms = torch.cuda.get_device_properties(m.RowWindowOffset.device).multi_processor_count
     G = min(grid if grid > 0 else 16 * sms, m.T)
-    return 2 if (mode == 1 and G > 1) else 1
+    return (1 if queue else 0) + 1 + (1 if (mode == 1 and G > 1) else 0)
 
 
 def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True, out=None,
             workspace=None, ntile=0):
-    if m.W != 8:
-        raise ValueError("the SpMM kernels take TC blocks of width 8")
+    """SpMM with any B storage form (planes from pack_b), precision and schedule
+    (mode 0 window / 1 balance, grid = chunks, ntile = 128-feature tiles per CTA),
+    on ME-TCF arrays of window height 16 or 32 and block width 8 (or 16 at height
+    16)."""
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     wsb = C.c_size_t()
@@ -178,7 +183,7 @@ def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True
         ws = torch.empty(wsb.value, dtype=torch.uint8, device=dev)
     vals = m.TCvalues if use_values else None
     call("dtc_spmm_ex", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId), _ptr(m.TCblockoffset),
-         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt, _ptr(planes[0]),
+         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, m.W, fmt, _ptr(planes[0]),
          _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(C_), mode, grid,
          ntile, _ptr(ws), 0 if ws is None else ws.numel(), _stream())
     return C_
@@ -187,8 +192,6 @@ def spmm_ex(m: METCF, planes, fmt, N, precision, mode=0, grid=0, use_values=True
 def spmm_fused(m: METCF, planes, fmt, N, precision, bias=None, relu=False, mode=0, grid=0,
                ntile=0, use_values=True, out=None, workspace=None):
     """spmm_ex with C = act(A*B + bias) fused into the store of C (GCN epilogue)."""
-    if m.W != 8:
-        raise ValueError("the SpMM kernels take TC blocks of width 8")
     dev = planes[0].device
     C_ = out if out is not None else torch.empty((m.M, N), dtype=torch.float32, device=dev)
     wsb = C.c_size_t()
@@ -199,7 +202,7 @@ def spmm_fused(m: METCF, planes, fmt, N, precision, bias=None, relu=False, mode=
     vals = m.TCvalues if use_values else None
     bias = None if bias is None else bias.to(torch.float32).contiguous()
     call("dtc_spmm_fused", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId),
-         _ptr(m.TCblockoffset), _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt,
+         _ptr(m.TCblockoffset), _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, m.W, fmt,
          _ptr(planes[0]), _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(bias),
          1 if relu else 0, _ptr(C_), mode, grid, ntile, _ptr(ws), 0 if ws is None else ws.numel(),
          _stream())

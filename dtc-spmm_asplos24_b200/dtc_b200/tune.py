@@ -59,7 +59,7 @@ def autotune(m: METCF, planes, fmt, N, precision, reps=3, use_values=True, out=N
     nres, best = C.c_int(), C.c_int()
     vals = m.TCvalues if use_values else None
     call("dtc_autotune", _ptr(m.RowWindowOffset), _ptr(m.TCblocktileId), _ptr(m.TCblockoffset),
-         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, fmt, _ptr(planes[0]),
+         _ptr(m.SparseAToX), _ptr(vals), m.M, m.nwin, m.T, m.H, m.W, fmt, _ptr(planes[0]),
          _ptr(planes[1]) if len(planes) > 1 else None, N, precision, _ptr(C_), _ptr(ws),
          ws.numel(), reps, res, ncand, C.byref(nres), C.byref(best), _stream())
     out_list = list(res)[: nres.value]

@@ -8,7 +8,14 @@
  * *_workspace_bytes query. The tcgen05 SpMM entry points read B and write C
  * with 16-byte accesses and TMA stores: d_B / B planes and d_C must be 16-byte
  * aligned and N a multiple of 4 (16 for the split-precision forms); other N
- * go to the legacy-ISA kernel where an entry point says so.
+ * go to the legacy-ISA kernel where an entry point says so. They also read
+ * d_sparseAToX in 16-byte pieces: it must be 16-byte aligned.
+ *
+ * Workspaces of the SpMM entry points hold the partial tiles of strict balance
+ * (required) followed by a small chunk-queue region (optional): with it, one
+ * CTA per SM pulls chunks of TC blocks from a device counter; with only the
+ * required bytes, the kernels run one CTA per chunk. The *_workspace_bytes
+ * queries return the size with the queue (workspace base 256-byte aligned).
  *
  * Each entry point names the reference interface it replaces (paths relative
  * to the reference project root, HPMLL/DTC-SpMM_ASPLOS24).
@@ -225,20 +232,23 @@ dtc_status dtc_spmm_balance_noalloc(const int32_t* d_tcblockRowid, const uint8_t
 size_t dtc_noalloc_scratch_capacity(void);
 
 /* General form used by the tuned paths: any B format / precision, explicit
- * schedule. block_h = row-window height of the ME-TCF arrays (16 or 32; the
- * conversion's blockSize_h, with blockSize_w = 8). mode 0 = window-scheduled,
- * 1 = strict balance. grid = CTAs (0 = 16 per SM, run as waves). ntile =
- * 128-feature tiles per CTA (0 = all of N up to 4, or up to 2 for the split
- * forms at block_h 32; 1 or 2 split wider N across more CTAs).
- * d_rowWindowOffset is required (build it from TCblockRowid with
- * dtc_rowid_to_window_offset). Workspace needed only for mode 1. */
+ * schedule. block_h x block_w = the ME-TCF's block shape (the conversion's
+ * blockSize_h x blockSize_w, DTC-SpMM/DTCSpMM.cpp:315-316): 16 x 8, 32 x 8 or
+ * 16 x 16 (the compaction width knob; tile ids must fit a byte).
+ * mode 0 = window-scheduled, 1 = strict balance. grid = chunks G of the TC-block
+ * range (0 = 16 per SM); the split threshold is ceil(num_blocks / G) blocks.
+ * ntile = 128-feature tiles per CTA (0 = all of N up to 4, or up to 2 for the
+ * split forms at block_h 32 or block_w 16; 1 or 2 split wider N across more
+ * CTAs). d_rowWindowOffset is required (build it from TCblockRowid with
+ * dtc_rowid_to_window_offset). Workspace: required in mode 1 (partial tiles),
+ * optional chunk queue after it (see the top of this header). */
 dtc_status dtc_spmm_ex(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                        const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                        const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                       int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
-                       const void* d_Bplane1, int32_t N, int precision, float* d_C, int mode,
-                       int grid, int ntile, void* d_workspace, size_t workspace_bytes,
-                       dtc_stream_t stream);
+                       int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                       const void* d_Bplane0, const void* d_Bplane1, int32_t N, int precision,
+                       float* d_C, int mode, int grid, int ntile, void* d_workspace,
+                       size_t workspace_bytes, dtc_stream_t stream);
 dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, int32_t N,
                                        int32_t block_h, int mode, int grid, size_t* bytes);
 
@@ -249,10 +259,11 @@ dtc_status dtc_spmm_ex_workspace_bytes(int32_t num_nodes, int64_t num_blocks, in
 dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                           const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                           const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                          int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
-                          const void* d_Bplane1, int32_t N, int precision, const float* d_bias,
-                          int relu, float* d_C, int mode, int grid, int ntile, void* d_workspace,
-                          size_t workspace_bytes, dtc_stream_t stream);
+                          int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                          const void* d_Bplane0, const void* d_Bplane1, int32_t N, int precision,
+                          const float* d_bias, int relu, float* d_C, int mode, int grid,
+                          int ntile, void* d_workspace, size_t workspace_bytes,
+                          dtc_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
 /* Schedule autotuner. Replaces the reference's hand-written schedule table   */
@@ -261,10 +272,10 @@ dtc_status dtc_spmm_fused(const int32_t* d_rowWindowOffset, const uint8_t* d_til
 /* ------------------------------------------------------------------------- */
 typedef struct {
   int32_t mode;   /* 0 = window-scheduled (no window split), 1 = strict balance */
-  int32_t waves;  /* CTAs = waves x SMs, capped at T; in mode 1 the split       */
-                  /* threshold is ceil(T / CTAs) TC blocks per CTA             */
+  int32_t waves;  /* chunks = waves x SMs, capped at T: the split threshold is  */
+                  /* ceil(T / chunks) TC blocks (one CTA per SM pulls chunks)  */
   int32_t ntile;  /* 128-feature tiles per CTA (1, 2 or 4)                      */
-  int32_t grid;   /* CTA count the measurement used (output)                    */
+  int32_t grid;   /* chunk count the measurement used (output)                  */
   float ms;       /* mean kernel time over the timed repetitions (output)       */
 } dtc_schedule;
 
@@ -288,7 +299,8 @@ dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, i
 dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileId,
                         const int32_t* d_tcblockOffset, const int32_t* d_sparseAToX,
                         const float* d_tcValues, int32_t num_nodes, int32_t num_windows,
-                        int64_t num_blocks, int32_t block_h, int bformat, const void* d_Bplane0,
+                        int64_t num_blocks, int32_t block_h, int32_t block_w, int bformat,
+                        const void* d_Bplane0,
                         const void* d_Bplane1, int32_t N, int precision, float* d_C,
                         void* d_workspace, size_t workspace_bytes, int reps,
                         dtc_schedule* results, int max_results, int* num_results, int* best,
@@ -346,6 +358,16 @@ dtc_status dtc_mlp_adam(float* d_params, const float* d_grads, float* d_m, float
  * (feasible_per_row = 0) or one row per input (feasible_per_row = 1). */
 dtc_status dtc_mlp_argmin(const float* d_Y, const uint8_t* d_feasible, int feasible_per_row,
                           int32_t batch, int32_t out, int32_t* d_choice, dtc_stream_t stream);
+
+/* Per-CTA timing of the SpMM kernels, for load-balance analysis; off by
+ * default. While set on the current device (capacity > 0), every SpMM launch
+ * writes, for each of its CTAs c < capacity (c = blockIdx.x + gridDim.x *
+ * blockIdx.y), four uint64 values to d_records[4c .. 4c+3]: the %globaltimer
+ * (ns) at kernel entry and at exit, the SM id, and the number of TC-block
+ * chunks the CTA processed. capacity = 0 turns it off. No reference
+ * counterpart (the reference's per-SM clock kernels,
+ * DTC-SpMM/DTCSpMM_kernel.cu:62-79, are a separate instrumented build). */
+dtc_status dtc_set_cta_timer(uint64_t* d_records, int32_t capacity);
 
 /* d_rowWindowOffset[num_windows+1] from a sorted d_tcblockRowid[T]. */
 dtc_status dtc_rowid_to_window_offset(const int32_t* d_tcblockRowid, int64_t num_blocks,

@@ -52,8 +52,8 @@ def test_bad_arguments_return_status_not_exit():
     assert L.dtc_convert_workspace_bytes(10, 10, 32, 16, C.byref(n)) == 1  # 32*16 > 256
     assert L.dtc_bformat_bytes(99, 10, 10, C.byref(n), C.byref(n)) == 1
     assert L.dtc_spmm(None, None, None, None, None, 16, 1, 1, None, 16, None, None) == 1
-    assert L.dtc_spmm_ex(None, None, None, None, None, 16, 1, 1, 16, 0, None, None, 16, 0, None,
-                         7, 0, 0, None, 0, None) == 1
+    assert L.dtc_spmm_ex(None, None, None, None, None, 16, 1, 1, 16, 8, 0, None, None, 16, 0,
+                         None, 7, 0, 0, None, 0, None) == 1
 
 
 def test_bformat_sizes():

@@ -277,3 +277,63 @@ def test_rowid_to_window_offset_flags_bad_ids_and_stays_in_bounds(cuda, bad):
     assert rc == 0
     assert metcf.device_status(clear=True) & 2
     assert (buf[:32] == 12345).all() and (buf[32 + nwin + 1:] == 12345).all()
+
+
+def _long_hole(M=12000, seed=3):
+    """Rows 1000..8999 empty (a run of 500 empty 16-row windows, longer than the
+    kernels' window-record ring) plus scattered empty rows."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(M):
+        if 1000 <= i < 9000 or i % 17 == 5:
+            rows.append(np.zeros(0, np.int64))
+        else:
+            rows.append(np.sort(rng.choice(M, size=int(rng.integers(1, 30)), replace=False)))
+    rp = np.zeros(M + 1, np.int32)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate(rows).astype(np.int32)
+    val = rng.uniform(-1, 1, len(col)).astype(np.float32)
+    return rp, col, val, M
+
+
+@pytest.mark.parametrize("H", [16, 32])
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("grid", [0, 5, 148])
+def test_long_run_of_empty_windows(cuda, H, mode, grid):
+    import torch
+    from dtc_b200 import metcf, B_F32, B_BF16X2, PREC_TF32, PREC_SPLIT3
+    rp, col, val, M = _long_hole()
+    m = metcf.convert(rp, col, M, H=H, values=val)
+    N = 64
+    B = np.random.default_rng(4).standard_normal((M, N)).astype(np.float32)
+    Bt = torch.from_numpy(B).cuda()
+    ref = O.spmm_f64(rp, col, val, M, B)
+    bound = O.spmm_absbound_f64(rp, col, val, M, B)
+    for fmt, prec, tol in ((B_F32, PREC_TF32, TF32_TOL), (B_BF16X2, PREC_SPLIT3, 2.0 ** -14)):
+        planes = [Bt] if fmt == B_F32 else metcf.pack_b(Bt, fmt)
+        C = metcf.spmm_ex(m, planes, fmt, N, prec, mode=mode, grid=grid).cpu().numpy()
+        assert (np.abs(C.astype(np.float64) - ref) <= tol * bound + 1e-6).all()
+    assert metcf.device_status(clear=True) == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_chunk_queue_and_one_cta_per_chunk_agree_bitwise(cuda, mode):
+    """Persistent CTAs pulling chunks from the queue and one CTA per chunk give
+    the same bits: results depend only on the chunking."""
+    import torch
+    from dtc_b200 import gen, metcf, B_F32, B_BF16X2, PREC_TF32, PREC_SPLIT3
+    A = gen.rmat(14, 16.0, 0.57, 0.19, 0.19, seed=2)
+    for H in (16, 32):
+        m = metcf.convert(A.rowptr, A.col, A.M, H=H, values=A.val)
+        N = 128
+        Bt = torch.from_numpy(gen.normal(A.M, N, seed=1)).cuda()
+        for fmt, prec in ((B_F32, PREC_TF32), (B_BF16X2, PREC_SPLIT3)):
+            planes = [Bt] if fmt == B_F32 else metcf.pack_b(Bt, fmt)
+            full = metcf.spmm_ex_workspace_bytes(m, N, mode, 0)
+            queue = metcf.spmm_ex_workspace_bytes(m, N, 0, 0)  # the queue region alone
+            outs = []
+            for wsb in (full, full - queue):
+                ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device="cuda")
+                outs.append(metcf.spmm_ex(m, planes, fmt, N, prec, mode=mode, workspace=ws))
+            assert torch.equal(outs[0], outs[1])
+    assert metcf.device_status(clear=True) == 0
