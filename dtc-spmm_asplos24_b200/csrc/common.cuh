@@ -200,6 +200,11 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
           smem_u32(bar))
       : "memory");
 }
+// A UMMA descriptor from its two 32-bit words (start-address offsets only
+// change the low word: shared addresses < 256 KB never carry into the high one).
+__device__ __forceinline__ uint64_t desc_at(uint32_t lo, uint32_t hi) {
+  return ((uint64_t)hi << 32) | lo;
+}
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                          uint32_t idesc, uint32_t accumulate) {
   asm volatile(

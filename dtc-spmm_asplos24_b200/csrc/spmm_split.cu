@@ -67,6 +67,7 @@ struct SCfg {
   static constexpr bool kConv = (FORM == kFormSplit24 || FORM == kFormFP8);
   static constexpr int kThreads = 32 * (kConvWarp0 + (kConv ? kConvWarps : 0));
   static_assert(S % kLoadWarps == 0 && S % kTileWarps == 0 && S % kConvWarps == 0, "ownership");
+  static_assert((S & (S - 1)) == 0 && S % 2 == 0, "stage counters are kept modulo 2^32");
   static_assert(kConvWarps <= kEndStages, "end markers");
   static_assert(BW == 8 || BW == 16, "block width");
   static_assert(P * BW <= 32, "one SparseAToX entry per lane");
@@ -512,6 +513,8 @@ __global__ void __launch_bounds__(SCfg<FORM, NT, P, S, WH, BW>::kThreads, 1)
       constexpr uint32_t idesc = umma_idesc(1, 128, 2 * WH, 1, 0);
       const uint64_t adesc0 = umma_desc(smem_u32(xring), 1024, 2048, 2);
       const uint64_t bdesc0 = umma_desc(smem_u32(yring), 128, 256, 0);
+      const uint32_t adesc_lo = (uint32_t)adesc0, adesc_hi = (uint32_t)(adesc0 >> 32);
+      const uint32_t bdesc_lo = (uint32_t)bdesc0, bdesc_hi = (uint32_t)(bdesc0 >> 32);
       uint32_t q = 0;
       bool ok = true;
       for (uint32_t rq = 0; ok; ++rq) {
@@ -536,37 +539,41 @@ __global__ void __launch_bounds__(SCfg<FORM, NT, P, S, WH, BW>::kThreads, 1)
         uint32_t acc = 0;
         // this issuer's stages of the window, in order (stage g belongs to
         // issuer g % 2; chunks start on even stages, so the chunk-relative
-        // index has the same parity)
-        const int64_t rel_first = (rec.wb0 - rec.cb0) / P;
-        const int64_t rel_last = (rec.wb1 - 1 - rec.cb0) / P;
-        for (int64_t rel = rel_first + ((rel_first & 1) != m); rel <= rel_last; rel += kMmaWarps) {
-          const int64_t gst = rec.stage_base + rel;
-          const int s = (int)(gst % S);
-          const int64_t sb = rec.cb0 + rel * P;           // first block of the stage
-          const int64_t lo = sb > rec.wb0 ? sb : rec.wb0;
-          const int64_t hi = (sb + P) < rec.wb1 ? (sb + P) : rec.wb1;
-          const bool last = (hi == sb + P || hi == rec.cb1);  // stage fully consumed
-          if (lo == sb) {  // first visit of this stage (windows are walked in order)
-            if (!mbar_wait(&full[s], (uint32_t)(gst / S) & 1, p.err)) { ok = false; break; }
+        // index has the same parity). Indices relative to the chunk fit 32 bits
+        // (T < 2^31); the CTA's stage counter is kept modulo 2^32, which S divides.
+        const int32_t rb0 = (int32_t)(rec.wb0 - rec.cb0), rb1 = (int32_t)(rec.wb1 - rec.cb0);
+        const int32_t cbn = (int32_t)(rec.cb1 - rec.cb0);
+        int32_t rel = rb0 / P;
+        rel += (int32_t)((rel & 1) != m);
+        uint32_t g = (uint32_t)rec.stage_base + (uint32_t)rel;
+        for (int32_t sbr = rel * P; sbr < rb1; sbr += kMmaWarps * P, g += kMmaWarps) {
+          const int s = (int)(g % S);
+          const int32_t lo = sbr > rb0 ? sbr : rb0;
+          const int32_t hi = (sbr + P) < rb1 ? (sbr + P) : rb1;
+          if (lo == sbr) {  // first visit of this stage (windows are walked in order)
+            if (!mbar_wait(&full[s], (g / S) & 1, p.err)) { ok = false; break; }
             fence_proxy_async_smem();  // cp.async (generic proxy) data -> UMMA reads
             tc_fence_after();
           }
-          uint64_t bdesc = bdesc0 + (uint64_t)((s * K::kStageY + (int)(lo - sb) * K::kYB) >> 4);
-          uint64_t adesc = adesc0 + (uint64_t)((s * K::kStageX +
-                                                (int)(lo - sb) * NT * K::kSub * kTileBytes) >> 4);
-          for (int64_t b = lo; b < hi; ++b) {
+          uint32_t blo = bdesc_lo + (uint32_t)((s * K::kStageY + (lo - sbr) * K::kYB) >> 4);
+          uint32_t alo = adesc_lo + (uint32_t)((s * K::kStageX + (lo - sbr) * NT * K::kSub * kTileBytes) >> 4);
 #pragma unroll
-            for (int h = 0; h < K::kSub; ++h)
+          for (int j = 0; j < P; ++j) {
+            if (lo + j < hi) {
 #pragma unroll
-              for (int t = 0; t < NT; ++t)
-                mma_f16(dtm + t * 2 * WH,
-                        adesc + (uint64_t)(((t * K::kSub + h) * kTileBytes) >> 4),
-                        bdesc + (uint64_t)((h * K::kYB8) >> 4), idesc, h == 0 ? acc : 1u);
-            acc = 1;
-            adesc += (uint64_t)((NT * K::kSub * kTileBytes) >> 4);
-            bdesc += (uint64_t)(K::kYB >> 4);
+              for (int h = 0; h < K::kSub; ++h)
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                  mma_f16(dtm + t * 2 * WH,
+                           desc_at(alo + (uint32_t)(((t * K::kSub + h) * kTileBytes) >> 4), adesc_hi),
+                           desc_at(blo + (uint32_t)((h * K::kYB8) >> 4), bdesc_hi), idesc,
+                           h == 0 ? acc : 1u);
+              acc = 1;
+              alo += (uint32_t)((NT * K::kSub * kTileBytes) >> 4);
+              blo += (uint32_t)(K::kYB >> 4);
+            }
           }
-          if (last) tc_commit(&empty[s]);
+          if (hi == sbr + P || hi == cbn) tc_commit(&empty[s]);  // stage fully consumed
         }
         if (!ok) break;
         tc_commit(&acc_full[a]);
@@ -734,6 +741,7 @@ dtc_status spmm_split_impl(const int32_t* rwo, const uint8_t* tile, const int32_
                            cudaStream_t st, int ntile, Epilogue epi, int H, void* queue,
                            int W) {
   DTC_REQUIRE(M >= 0 && N >= 1 && T >= 0, "bad sizes");
+  DTC_REQUIRE(T < ((int64_t)1 << 31), "more than 2^31 - 1 TC blocks");
   DTC_REQUIRE(bformat == DTC_B_SPLIT24 || bformat == DTC_B_BF16 || bformat == DTC_B_FP8 ||
                   bformat == DTC_B_BF16X2,
               "split kernels take SPLIT24, BF16, FP8 or BF16X2 B");
