@@ -20,13 +20,13 @@
 // chunk-relative, so which CTA ran which chunk never changes a bit.
 //
 // Stage ownership. Stage g of a CTA (its g-th stage overall) sits in ring slot
-// g % S and belongs to UMMA issuer g % 2 (S is even, so each issuer only ever
-// meets its own slots, and only the owner waits on and releases a slot). Every
-// chunk starts on an even stage: when a chunk would start on an odd one, the
-// producer first emits a pad stage (no blocks) and a kRecPad record for it,
-// which its owner waits on and releases. Stage parity inside a chunk therefore
-// equals its parity inside the CTA's stream, whatever chunks the CTA ran
-// before.
+// g % S and belongs to UMMA issuer g % I, I the kernel's issuer count (S is a
+// multiple of I, so each issuer only ever meets its own slots, and only the
+// owner waits on and releases a slot). Every chunk starts on a multiple of I:
+// before a chunk that would start elsewhere, the producer emits pad stages (no
+// blocks) with one kRecPad record each, which their owners wait on and
+// release. A stage's issuer inside a chunk is therefore its chunk-relative
+// index % I, whatever chunks the CTA ran before.
 //
 // Producer warp. One warp walks the CTA's chunks ahead of everyone else:
 //   stage metadata  per stage of P consecutive blocks: first block, block
@@ -258,7 +258,7 @@ __device__ __forceinline__ void init_rings(const SchedRings& r, uint32_t meta_co
 // The producer warp (all 32 lanes). Emits, for every chunk this CTA takes,
 // its stages (P blocks of width BW each) and its window records, then
 // kEndStages end stages and one end record.
-template <int P, int BW>
+template <int P, int BW, int ALIGN>
 __device__ void produce(const Params& p, const SchedRings& r, int lane,
                         volatile uint32_t* abort_flag) {
   uint64_t gst = 0;   // stages emitted
@@ -397,11 +397,12 @@ __device__ void produce(const Params& p, const SchedRings& r, int lane,
     const bool last_chunk = (kc == p.G - 1);
     if (cb0 >= cb1 && !last_chunk) continue;
     rec_cb1 = cb1;
-    if ((gst & 1) && cb0 < cb1) {  // pad stage: the chunk starts on an even stage
+    while (ok && (gst % ALIGN) != 0 && cb0 < cb1) {  // pad stages: align the chunk's start
       const int64_t pad_stage = (int64_t)gst;
       if (!emit_stages(cb0, 1, cb1, 0)) break;
       emit_rec(-1, cb0, cb0, cb0, pad_stage, kc, kRecPad);
     }
+    if (!ok) break;
     const int64_t sbase = (int64_t)gst;
     int32_t wcur = -1;     // current nonempty window
     int64_t wend = cb0;    // its end (block)

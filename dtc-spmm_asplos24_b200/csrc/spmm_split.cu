@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(SCfg<FORM, NT, P, S, WH, BW>::kThreads, 1)
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == kProdWarp) {
-    produce<P, BW>(p, rings, lane, abort_flag);
+    produce<P, BW, kMmaWarps>(p, rings, lane, abort_flag);
   } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ------------------------------------------------------------ loaders
     const int lw = warp - kLoadWarp0;
@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(SCfg<FORM, NT, P, S, WH, BW>::kThreads, 1)
         uint32_t acc = 0;
         // this issuer's stages of the window, in order (stage g belongs to
         // issuer g % 2; chunks start on even stages, so the chunk-relative
-        // index has the same parity). Indices relative to the chunk fit 32 bits
+        // index gives the same issuer). Indices relative to the chunk fit 32 bits
         // (T < 2^31); the CTA's stage counter is kept modulo 2^32, which S divides.
         const int32_t rb0 = (int32_t)(rec.wb0 - rec.cb0), rb1 = (int32_t)(rec.wb1 - rec.cb0);
         const int32_t cbn = (int32_t)(rec.cb1 - rec.cb0);

@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const __grid_constant
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == kProdWarp) {
-    produce<P, BW>(p, rings, lane, abort_flag);
+    produce<P, BW, kMmaWarps>(p, rings, lane, abort_flag);
   } else if (warp >= kLoadWarp0 && warp < kLoadWarp0 + kLoadWarps) {
     // ------------------------------------------------------------ loaders
     const int lw = warp - kLoadWarp0;

@@ -7,8 +7,10 @@
 //   mode   0 = window-scheduled (windows never split), 1 = strict balance
 //          (windows longer than the per-CTA chunk are split; the chunk,
 //          ceil(T / grid) blocks, is the split threshold)
-//   waves  CTAs = waves x SMs (one resident CTA per SM; more waves = smaller
-//          ranges, which evens out skew at the price of more range setup)
+//   waves  chunks = waves x SMs, pulled by one persistent CTA per SM from a
+//          device counter (more chunks even out skew at the price of more
+//          chunk boundaries); window mode also tries 32 and 64, balance mode,
+//          whose cut windows need partial tiles per chunk, stops at 16
 //   ntile  128-feature tiles per CTA (fewer tiles spread wide N over more CTAs)
 // Each candidate runs once untimed and `reps` times between CUDA events on the
 // caller's stream; the mean is its time. Candidates change neither the B form
@@ -23,8 +25,9 @@ using namespace dtc;
 
 namespace {
 
-constexpr int kWaveChoices[] = {1, 2, 4, 8, 16};
-constexpr int kMaxWaves = 16;
+constexpr int kWaveChoices[] = {1, 2, 4, 8, 16, 32, 64};
+constexpr int kMaxWaves = 64;         // chunks of the queue region
+constexpr int kMaxBalanceWaves = 16;  // chunks with partial tiles (balance mode)
 
 // N-tiles per CTA when the caller does not cap them (see the kernels' dispatch).
 int auto_ntile(int32_t N, int H, bool split) {
@@ -39,6 +42,7 @@ int candidates(int32_t N, int H, bool split, dtc_schedule* out, int max) {
   for (int mode = 0; mode <= 1; ++mode)
     for (int w : kWaveChoices)
       for (int nt = 1; nt <= 4; nt *= 2) {
+        if (mode == 1 && w > kMaxBalanceWaves) break;
         if (nt > nt_auto) break;
         if (out && n < max) {
           dtc_schedule& s = out[n];
@@ -81,7 +85,7 @@ dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, i
   DTC_REQUIRE(bytes != nullptr, "bytes is null");
   DTC_REQUIRE(num_nodes >= 0 && num_blocks >= 0 && N >= 1, "bad sizes");
   DTC_REQUIRE(block_h == 16 || block_h == 32, "block_h must be 16 or 32");
-  *bytes = align_up(spmm_partials_bytes(num_blocks, N, kMaxWaves * num_sms(), block_h), 256) +
+  *bytes = align_up(spmm_partials_bytes(num_blocks, N, kMaxBalanceWaves * num_sms(), block_h), 256) +
            spmm_queue_bytes(num_blocks, kMaxWaves * num_sms());
   return DTC_OK;
 }
@@ -123,7 +127,7 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
   // the chunk queue sits after the largest candidate's partial tiles
   void* queue = queue_region(
       d_workspace, workspace_bytes,
-      align_up(spmm_partials_bytes(num_blocks, N, kMaxWaves * sms, block_h), 256), num_blocks,
+      align_up(spmm_partials_bytes(num_blocks, N, kMaxBalanceWaves * sms, block_h), 256), num_blocks,
       kMaxWaves * sms);
   int best_i = -1;
   for (int i = 0; i < ncand; ++i) {

@@ -301,7 +301,9 @@ def measure(spec, reps=3, device="cuda"):
                 scheds, _ = tune.autotune(mm, planes[fo], fmt, N, prec, reps=reps, out=out,
                                           workspace=ws)
                 for s in scheds:
-                    times[class_of(s.mode, s.waves, s.ntile, fo, ro, h)] = s.ms
+                    key = (s.mode, s.waves, s.ntile, fo, ro, h)
+                    if key in _INDEX:  # schedules outside the class space are not labels
+                        times[_INDEX[key]] = s.ms
             del ws, mm
     return feat, times, info
 
@@ -456,8 +458,10 @@ class Scheduler:
                 for fo in FORMS:
                     fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
                     scheds, b = tune.autotune(mm, metcf.pack_b(B, fmt), fmt, N, prec, reps=reps)
-                    if best is None or b.ms < best:
-                        best, best_c = b.ms, class_of(b.mode, b.waves, b.ntile, fo, ro, h)
+                    for sc in scheds:  # the fastest schedule inside the class space
+                        key = (sc.mode, sc.waves, sc.ntile, fo, ro, h)
+                        if key in _INDEX and (best is None or sc.ms < best):
+                            best, best_c = sc.ms, _INDEX[key]
         return best_c
 
 

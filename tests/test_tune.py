@@ -10,12 +10,13 @@ from dtc_b200 import tune
 
 def test_candidates_cover_modes_waves_ntiles():
     c128 = tune.candidates(128)
-    assert len(c128) == 2 * 5  # mode x waves, one N-tile
+    assert len(c128) == 7 + 5  # window mode 7 wave counts, balance mode 5; one N-tile
     assert {s.mode for s in c128} == {0, 1}
-    assert {s.waves for s in c128} == {1, 2, 4, 8, 16}
+    assert {s.waves for s in c128 if s.mode == 0} == {1, 2, 4, 8, 16, 32, 64}
+    assert {s.waves for s in c128 if s.mode == 1} == {1, 2, 4, 8, 16}
     assert {s.ntile for s in c128} == {1}
     c512 = tune.candidates(512)
-    assert len(c512) == 2 * 5 * 3
+    assert len(c512) == (7 + 5) * 3
     assert {s.ntile for s in c512} == {1, 2, 4}
     assert len({s.key() for s in c512}) == len(c512)
     assert tune.candidates(0) == []
