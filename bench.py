@@ -631,13 +631,13 @@ def main():
     shape_name = lambda hw: f"h{hw[0]}w{hw[1]}"
     exh_key = min((k for k in tuned_tbl if k[0] != "tf32"), key=lambda k: tuned_tbl[k].ms)
 
-    # the learned scheduler's choice (features -> MLP on the GPU, its 4 cheapest
+    # the learned scheduler's choice (features -> MLP on the GPU, its 8 cheapest
     # predicted classes timed on this matrix); the exhaustive autotuner is its
     # fallback when no weights match the class space
     t0 = time.perf_counter()
     plan = costmodel.Scheduler(device=dev).plan(torch.from_numpy(A.rowptr).to(dev),
                                                 torch.from_numpy(A.col).to(dev), m, N, B=B,
-                                                verify_top=4)
+                                                verify_top=8)
     plan_s = time.perf_counter() - t0
     perm = None
     At = A

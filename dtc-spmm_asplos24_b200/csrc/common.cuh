@@ -1,5 +1,5 @@
 // Shared device/host helpers for the sm_100a kernels: status handling, bounded
-// mbarrier waits, TMA (tile::gather4) loads and tcgen05 (TMEM / UMMA) wrappers.
+// mbarrier waits, TMA stores and tcgen05 (TMEM / UMMA) wrappers.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda.h>
@@ -154,24 +154,6 @@ __device__ __forceinline__ void named_bar_sync(uint32_t id, uint32_t count) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// TMA 2-D tile::gather4: four rows (r0..r3) of `box` width starting at column
-// `x` (x * element size must be a multiple of 16 bytes) into consecutive
-// 128-byte smem rows at `dst`; completes `bytes` on `bar`. Rows outside the
-// tensor are zero-filled.
-__device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int32_t x, int32_t r0, int32_t r1, int32_t r2,
-                                            int32_t r3) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(r0), "r"(r1),
-      "r"(r2), "r"(r3)
-      : "memory");
-}
-
-__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
-  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
-}
 
 // ---- tcgen05 -------------------------------------------------------------
 __device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols) {

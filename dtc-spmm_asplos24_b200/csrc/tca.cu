@@ -173,10 +173,27 @@ __global__ void k_pair_jaccard(const uint64_t* __restrict__ pairs, int64_t np,
 }
 
 // Device workspace for one level over n items with P-value signatures.
+// Workspace of one banding + scoring pass. The distinct pair keys (pairs_in)
+// live through both stages; the banding stage's buffers (band keys, raw pairs,
+// their sort) are dead once the distinct pairs are known, so the scoring stage
+// (scores, order, its sort) reuses the same bytes: the pass needs the larger
+// stage, not their sum.
 struct LshLayout {
   size_t keys_in, keys_out, items_in, items_out, counts, offs, pairs_in, pairs_out, sort1, scan,
-      sort2, uniq, nsel, score_in, score_out, ord_in, ord_out, sort3, total;
+      sort2, uniq, uniq_bytes, nsel, score_in, score_out, ord_in, ord_out, sort3, sort3_bytes, total;
 };
+
+// skey[j] = keys[ord[j]] (the pairs in score order) and rank[ord[j]] = j (the
+// position of keys[i] in that order).
+__global__ void k_score_order(const uint64_t* __restrict__ keys, const int32_t* __restrict__ ord,
+                              int64_t n, uint64_t* __restrict__ skey, int32_t* __restrict__ rank) {
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += stride) {
+    const int32_t o = ord[j];
+    skey[j] = keys[o];
+    rank[o] = (int32_t)j;
+  }
+}
 
 // ord[i] = i.
 __global__ void k_iota(int32_t* __restrict__ ord, int64_t n) {
@@ -191,13 +208,16 @@ LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
   auto take = [&](size_t b) { size_t o = off; off = align_up(off + (b ? b : 1), 256); return o; };
   const size_t n = (size_t)(n_keys > 0 ? n_keys : 1);
   const size_t mp = (size_t)(max_pairs > 0 ? max_pairs : 1);
+  L.pairs_in = take(mp * 8);
+  L.nsel = take(8);
+  const size_t stage_base = off;
+  // banding stage
   L.keys_in = take(n * 8);
   L.keys_out = take(n * 8);
   L.items_in = take(n * 4);
   L.items_out = take(n * 4);
   L.counts = take((n + 1) * 4);
   L.offs = take((n + 1) * 4);
-  L.pairs_in = take(mp * 8);
   L.pairs_out = take(mp * 8);
   size_t s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, s1, (uint64_t*)nullptr, (uint64_t*)nullptr,
@@ -212,13 +232,17 @@ LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
   L.scan = take(s2);
   L.sort2 = take(s3);
   L.uniq = take(s5);
-  L.nsel = take(8);
+  L.uniq_bytes = s5;
+  const size_t banding_end = off;
+  // scoring stage, over the banding stage's bytes
+  off = stage_base;
   L.score_in = take(mp * 8);
   L.score_out = take(mp * 8);
   L.ord_in = take(mp * 4);
   L.ord_out = take(mp * 4);
   L.sort3 = take(s4);
-  L.total = off;
+  L.sort3_bytes = s4;
+  L.total = off > banding_end ? off : banding_end;
   return L;
 }
 
@@ -226,9 +250,10 @@ LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
 // order, their Jaccard scores, and the order of descending score (ties in
 // ascending pair order).
 struct Scored {
-  std::vector<uint64_t> keys;
-  std::vector<int32_t> order;   // indices into keys, best first
-  std::vector<double> score;    // score of keys[order[j]]
+  std::vector<uint64_t> keys;   // ascending
+  std::vector<uint64_t> skey;   // the same pairs, best score first
+  std::vector<double> score;    // score of skey[j]
+  std::vector<int32_t> rank;    // position of keys[i] in skey
 };
 
 // Candidate pairs for n items whose sorted, distinct sets are d_ptr / d_idx
@@ -237,8 +262,9 @@ dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, 
                      const LshLayout& L, int64_t max_pairs, const int64_t* d_ptr,
                      const int32_t* d_idx, cudaStream_t st, Scored& out) {
   out.keys.clear();
-  out.order.clear();
+  out.skey.clear();
   out.score.clear();
+  out.rank.clear();
   if (n < 2) return DTC_OK;
   const int64_t nk = (int64_t)n * prm.bands;
   uint64_t* kin = (uint64_t*)(ws + L.keys_in);
@@ -271,7 +297,7 @@ dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, 
   size_t b3 = L.uniq - L.sort2;
   DTC_CUDA(cub::DeviceRadixSort::SortKeys(ws + L.sort2, b3, pin, pout, (int64_t)np, 0, 64, st));
   int64_t* nsel = (int64_t*)(ws + L.nsel);
-  size_t b4 = L.nsel - L.uniq;
+  size_t b4 = L.uniq_bytes;
   DTC_CUDA(cub::DeviceSelect::Unique(ws + L.uniq, b4, pout, pin, nsel, (int64_t)np, st));
   int64_t nu = 0;
   DTC_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
@@ -283,15 +309,22 @@ dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, 
   k_pair_jaccard<<<grid_for(nu), kThreads, 0, st>>>(pin, nu, d_ptr, d_idx, sin);
   k_iota<<<grid_for(nu), kThreads, 0, st>>>(oin, nu);
   DTC_CUDA(cudaGetLastError());
-  size_t b5 = L.total - L.sort3;
+  size_t b5 = L.sort3_bytes;
   DTC_CUDA(cub::DeviceRadixSort::SortPairsDescending(ws + L.sort3, b5, sin, sout, oin, oout, nu,
                                                      0, 64, st));
+  // the sort's inputs are dead: score order of the keys into sin, ranks into oin
+  uint64_t* skey = (uint64_t*)sin;
+  int32_t* rank = oin;
+  k_score_order<<<grid_for(nu), kThreads, 0, st>>>(pin, oout, nu, skey, rank);
+  DTC_CUDA(cudaGetLastError());
   out.keys.resize(nu);
-  out.order.resize(nu);
+  out.skey.resize(nu);
   out.score.resize(nu);
+  out.rank.resize(nu);
   DTC_CUDA(cudaMemcpyAsync(out.keys.data(), pin, (size_t)nu * 8, cudaMemcpyDeviceToHost, st));
-  DTC_CUDA(cudaMemcpyAsync(out.order.data(), oout, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaMemcpyAsync(out.skey.data(), skey, (size_t)nu * 8, cudaMemcpyDeviceToHost, st));
   DTC_CUDA(cudaMemcpyAsync(out.score.data(), sout, (size_t)nu * 8, cudaMemcpyDeviceToHost, st));
+  DTC_CUDA(cudaMemcpyAsync(out.rank.data(), rank, (size_t)nu * 4, cudaMemcpyDeviceToHost, st));
   DTC_CUDA(cudaStreamSynchronize(st));
   return DTC_OK;
 }
@@ -329,8 +362,9 @@ struct QItem {
 };
 
 // The greedy merge loop; returns the root of every item. The initial pairs
-// come sorted (Scored); requeued (root, root) pairs go to a heap, and the next
-// pair is the better of the two heads in the QItem order.
+// come in score order (Scored::skey, walked front to back); requeued (root,
+// root) pairs go to a heap, and the next pair is the better of the two heads
+// in the QItem order.
 std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n, int32_t cap) {
   std::vector<int32_t> parent(n), size(n, 1);
   std::vector<char> deleted(n, 0);
@@ -346,15 +380,21 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n,
     return a < b ? ((uint64_t)a << 32) | (uint32_t)b : ((uint64_t)b << 32) | (uint32_t)a;
   };
   const int64_t np = (int64_t)sp.keys.size();
-  std::vector<int32_t> rank(np);  // position of keys[t] in the sorted order
-  for (int64_t j = 0; j < np; ++j) rank[sp.order[j]] = (int32_t)j;
+  const std::vector<int32_t>& rank = sp.rank;  // position of keys[t] in the score order
+  // The keys are sorted, so the initial pairs whose smaller member is a sit
+  // in [first[a], first[a + 1]): the queued test searches only those.
+  std::vector<int64_t> first((size_t)n + 1, 0);
+  for (int64_t j = 0; j < np; ++j) ++first[(size_t)(sp.keys[j] >> 32) + 1];
+  for (int32_t a = 0; a < n; ++a) first[a + 1] += first[a];
   int64_t next = 0;  // initial pairs before `next` have been popped
   std::priority_queue<QItem> q;
   std::unordered_set<uint64_t> requeued;  // pairs currently in the heap
   // a pair is queued when it is an initial pair not popped yet, or in the heap
   auto queued = [&](uint64_t k) {
-    const auto it = std::lower_bound(sp.keys.begin(), sp.keys.end(), k);
-    if (it != sp.keys.end() && *it == k && rank[it - sp.keys.begin()] >= next) return true;
+    const size_t a = (size_t)(k >> 32);
+    const auto b = sp.keys.begin() + first[a], e = sp.keys.begin() + first[a + 1];
+    const auto it = std::lower_bound(b, e, k);
+    if (it != e && *it == k && rank[it - sp.keys.begin()] >= next) return true;
     return requeued.count(k) > 0;
   };
   int64_t num_cluster = n;
@@ -362,7 +402,7 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n,
     QItem it;
     bool from_init;
     if (next < np) {
-      const uint64_t k0 = sp.keys[sp.order[next]];
+      const uint64_t k0 = sp.skey[next];
       const QItem a{sp.score[next], (int32_t)(k0 >> 32), (int32_t)(k0 & 0xffffffffu)};
       from_init = q.empty() || !(a < q.top());
       it = from_init ? a : q.top();

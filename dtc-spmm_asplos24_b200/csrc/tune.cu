@@ -116,9 +116,16 @@ dtc_status dtc_autotune(const int32_t* d_rowWindowOffset, const uint8_t* d_tileI
   } else {
     DTC_REQUIRE(N % 16 == 0, "split-precision path needs N % 16 == 0");
   }
-  const int ncand = candidates(N, block_h, !tf32, nullptr, 0);
-  std::vector<dtc_schedule> cand(ncand);
-  candidates(N, block_h, !tf32, cand.data(), ncand);
+  const int ncand_all = candidates(N, block_h, !tf32, nullptr, 0);
+  std::vector<dtc_schedule> cand(ncand_all);
+  candidates(N, block_h, !tf32, cand.data(), ncand_all);
+  if (!tf32 && block_w == 16) {  // the split kernels hold at most 2 N-tiles at width 16
+    std::vector<dtc_schedule> kept;
+    for (const dtc_schedule& c : cand)
+      if (c.ntile <= 2) kept.push_back(c);
+    cand.swap(kept);
+  }
+  const int ncand = (int)cand.size();
   cudaStream_t st = (cudaStream_t)stream;
   Events ev;
   DTC_CUDA(cudaEventCreate(&ev.a));

@@ -6,10 +6,11 @@ The reference fixes its schedule by hand per dataset and N
 
     (window height, compaction width, mode, waves, N-tile, B form, reorder)
 
-with row windows of 16 or 32 rows and TC blocks 8 columns wide (the kernels'
-compaction width), mode 0 (window-scheduled) or 1 (strict
-balance; the split threshold is ceil(T / CTAs) blocks), waves in {1,2,4,8,16}
-(CTAs = waves x SMs), N-tiles per CTA in {1,2,4}, two B forms within 1e-5
+with TC blocks of 16 x 8, 32 x 8 or 16 x 16 (window height x compaction width;
+the reference's blockSize_h x blockSize_w), mode 0 (window-scheduled) or 1
+(strict balance), waves in {1,2,4,8,16,32,64} in window mode and {1,2,4,8,16}
+in balance mode (chunks = waves x SMs, so the split threshold is ceil(T /
+chunks) blocks), N-tiles per CTA in {1,2,4}, two B forms within 1e-5
 relative error (SPLIT24, 3 bytes per element rebuilt on chip, and BF16X2, 4
 bytes per element used as stored; both with 3-term products) and TCA reorder off or
 on. The network predicts, for every class, log(t_class / t_best) of the SpMM
@@ -34,12 +35,12 @@ from ._lib import MlpDims, call
 from .metcf import _ptr, _stream
 
 NFEAT = 48
-HEIGHTS = (16, 32)
-WAVES = (1, 2, 4, 8, 16)
+SHAPES = ((16, 8), (32, 8), (16, 16))  # (window height, compaction width)
+WAVES = {0: (1, 2, 4, 8, 16, 32, 64), 1: (1, 2, 4, 8, 16)}  # per mode
 NTILES = (1, 2, 4)
 FORMS = ("split24x3", "bf16x2x3")
-CLASSES = [dict(H=h, W=8, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
-           for ro in (0, 1) for h in HEIGHTS for fo in FORMS for mo in (0, 1) for wv in WAVES
+CLASSES = [dict(H=h, W=w, mode=mo, waves=wv, ntile=nt, form=fo, reorder=ro)
+           for ro in (0, 1) for h, w in SHAPES for fo in FORMS for mo in (0, 1) for wv in WAVES[mo]
            for nt in NTILES]
 K = len(CLASSES)
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
@@ -47,29 +48,30 @@ DATASET_PATH = os.path.join(DATA_DIR, "costmodel_dataset.npz")
 WEIGHTS_PATH = os.path.join(DATA_DIR, "costmodel_weights.npz")
 
 
-def auto_ntile(N, H=16):
-    """N-tiles per CTA the split kernels use when uncapped (2 at most at H = 32)."""
+def auto_ntile(N, H=16, W=8):
+    """N-tiles per CTA the split kernels use when uncapped (2 at most at window
+    height 32 or compaction width 16)."""
     nt = 1 if N <= 128 else 2 if N <= 256 else 4
-    return min(nt, 2) if H == 32 else nt
+    return min(nt, 2) if (H == 32 or W == 16) else nt
 
 
 def feasible(N):
     """uint8 [K]: classes whose N-tile the kernels run for width N."""
-    return np.array([c["ntile"] <= auto_ntile(N, c["H"]) for c in CLASSES], np.uint8)
+    return np.array([c["ntile"] <= auto_ntile(N, c["H"], c["W"]) for c in CLASSES], np.uint8)
 
 
-_INDEX = {(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"]): i
+_INDEX = {(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"], c["W"]): i
           for i, c in enumerate(CLASSES)}
 
 
-def class_of(mode, waves, ntile, form, reorder, H=16):
-    return _INDEX[(mode, waves, ntile, form, reorder, H)]
+def class_of(mode, waves, ntile, form, reorder, H=16, W=8):
+    return _INDEX[(mode, waves, ntile, form, reorder, H, W)]
 
 
 def default_class(N):
     """The untuned library default for width N (window height 16, strict
     balance, 16 waves, all N-tiles in one CTA, SPLIT24 3-term, no reorder)."""
-    return class_of(1, 16, auto_ntile(N), "split24x3", 0, 16)
+    return class_of(1, 16, auto_ntile(N), "split24x3", 0, 16, 8)
 
 
 # ----------------------------------------------------------------- features
@@ -280,6 +282,7 @@ def measure(spec, reps=3, device="cuda"):
     feat = features(rp, cl, m, N).cpu().numpy()
     B = torch.from_numpy(gen.normal(A.M, N, seed=spec["seed"] + 2)).to(device)
     times = np.full(K, np.nan, np.float32)
+    feas = feasible(int(spec["N"])).astype(bool)
     info = dict(M=A.M, nnz=int(cl.numel()), T0=m.T)
     out = torch.empty((A.M, N), dtype=torch.float32, device=device)
     planes = {fo: metcf.pack_b(B, tune.FORMS[fo][0]) for fo in FORMS}
@@ -291,38 +294,67 @@ def measure(spec, reps=3, device="cuda"):
             torch.cuda.synchronize()
             info["tca_s"] = time.perf_counter() - t0
             src = (rp2, c2, v2)
-        for h in HEIGHTS:
-            mm = m if (h == 16 and not ro) else metcf.convert(src[0], src[1], A.M, H=h,
-                                                              values=src[2])
-            info[f"T_r{ro}_h{h}"] = mm.T
+        for h, w in SHAPES:
+            mm = m if ((h, w) == (16, 8) and not ro) else metcf.convert(src[0], src[1], A.M, H=h,
+                                                                        W=w, values=src[2])
+            info[f"T_r{ro}_h{h}w{w}"] = mm.T
             ws = tune.workspace_for(mm, N, B.device)
             for fo in FORMS:
                 fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
                 scheds, _ = tune.autotune(mm, planes[fo], fmt, N, prec, reps=reps, out=out,
                                           workspace=ws)
                 for s in scheds:
-                    key = (s.mode, s.waves, s.ntile, fo, ro, h)
-                    if key in _INDEX:  # schedules outside the class space are not labels
+                    key = (s.mode, s.waves, s.ntile, fo, ro, h, w)
+                    if key in _INDEX and feas[_INDEX[key]]:  # labels inside the class space
                         times[_INDEX[key]] = s.ms
             del ws, mm
     return feat, times, info
 
 
-def collect(n_train, n_test, seed=0, nnz_lo=2 ** 18, nnz_hi=2 ** 22, reps=3, log=None):
-    """Measured dataset over seeded synthetic matrices (train, then held-out)."""
+def collect(n_train, n_test, seed=0, nnz_lo=1e6, nnz_hi=3e7, reps=3, log=None, lo=0, hi=None,
+            checkpoint=None):
+    """Measured dataset over seeded synthetic matrices (train, then held-out).
+
+    The matrix list depends only on the seed and the counts, so [lo, hi) picks
+    a slice that can be measured in a separate run and merged later; with
+    `checkpoint` the slice measured so far is saved after every matrix. A
+    matrix whose measurement fails (a workspace beyond device memory) is
+    logged and left out."""
     rng = np.random.default_rng(seed)
     specs = [sample_spec(rng, nnz_lo, nnz_hi) for _ in range(n_train + n_test)]
+    hi = len(specs) if hi is None else min(hi, len(specs))
     F, Tm, meta = [], [], []
-    for i, sp in enumerate(specs):
+    for i in range(lo, hi):
+        sp = specs[i]
         t0 = time.perf_counter()
-        f, t, info = measure(sp, reps=reps)
+        try:
+            f, t, info = measure(sp, reps=reps)
+        except (torch.OutOfMemoryError, RuntimeError) as e:  # e.g. a workspace above device memory
+            torch.cuda.empty_cache()
+            if log:
+                log(f"[{i + 1}/{len(specs)}] {sp['family']} skipped: {str(e).splitlines()[0][:160]}")
+            continue
         F.append(f)
         Tm.append(t)
-        meta.append(dict(sp, **info, split="train" if i < n_train else "test"))
+        meta.append(dict(sp, **info, index=i, split="train" if i < n_train else "test"))
         if log:
             log(f"[{i + 1}/{len(specs)}] {sp['family']} N={sp['N']} nnz={info['nnz']} "
                 f"best={np.nanmin(t):.3f}ms {time.perf_counter() - t0:.1f}s")
+        if checkpoint:
+            save_dataset(dict(features=np.stack(F), times=np.stack(Tm), meta=meta), checkpoint)
     return dict(features=np.stack(F), times=np.stack(Tm), meta=meta)
+
+
+def merge(parts):
+    """One dataset from slices measured separately (ordered by matrix index);
+    times of classes infeasible for a matrix's N are set to NaN."""
+    F = np.concatenate([p["features"] for p in parts])
+    Tm = np.concatenate([p["times"] for p in parts]).astype(np.float64)
+    meta = sum((p["meta"] for p in parts), [])
+    for i, m in enumerate(meta):
+        Tm[i, ~feasible(int(m["N"])).astype(bool)] = np.nan
+    order = np.argsort([m["index"] for m in meta], kind="stable")
+    return dict(features=F[order], times=Tm[order], meta=[meta[i] for i in order])
 
 
 def save_dataset(ds, path=DATASET_PATH):
@@ -361,6 +393,7 @@ def fit(ds, steps=3000, lr=2e-3, seed=0, device="cuda"):
 class Plan:
     cls: int
     H: int
+    W: int
     form: str
     reorder: bool
     mode: int
@@ -383,7 +416,7 @@ class Scheduler:
              verify_top=0):
         """The class to run. With verify_top = k > 1 the model's k cheapest
         predicted classes are timed on the caller's data and the fastest wins
-        (model-guided search: k measurements instead of the exhaustive 240)."""
+        (model-guided search: k measurements instead of all K classes)."""
         if self.net is not None and not exhaustive:
             f = features(rowptr, col, m, N).reshape(1, -1)
             if verify_top > 1:
@@ -400,8 +433,8 @@ class Scheduler:
             c = self._exhaustive(rowptr, col, m, N, B, reps)
             src = "exhaustive"
         k = CLASSES[c]
-        return Plan(c, k["H"], k["form"], bool(k["reorder"]), k["mode"], k["waves"], k["ntile"],
-                    src)
+        return Plan(c, k["H"], k["W"], k["form"], bool(k["reorder"]), k["mode"], k["waves"],
+                    k["ntile"], src)
 
     @staticmethod
     def _fastest(rowptr, col, m, N, B, reps, classes):
@@ -414,16 +447,16 @@ class Scheduler:
         out = torch.empty((m.M, N), dtype=torch.float32, device=dev)
         for c in classes:
             k = CLASSES[c]
-            key = (k["reorder"], k["H"])
+            key = (k["reorder"], k["H"], k["W"])
             if key not in mets:
                 if k["reorder"]:
                     if "p" not in perms:
                         perms["p"] = reorder_mod.reorder(rowptr.to(dev), col.to(dev), None, m.M)
                     _, rp2, c2, _ = perms["p"]
-                    mets[key] = metcf.convert(rp2, c2, m.M, H=k["H"])
+                    mets[key] = metcf.convert(rp2, c2, m.M, H=k["H"], W=k["W"])
                 else:
-                    mets[key] = m if k["H"] == m.H else metcf.convert(rowptr.to(dev),
-                                                                      col.to(dev), m.M, H=k["H"])
+                    mets[key] = m if (k["H"], k["W"]) == (m.H, m.W) else metcf.convert(
+                        rowptr.to(dev), col.to(dev), m.M, H=k["H"], W=k["W"])
             mm = mets[key]
             fmt, prec = tune.FORMS[k["form"]][0], tune.FORMS[k["form"]][1]
             planes = metcf.pack_b(B, fmt)
@@ -453,36 +486,48 @@ class Scheduler:
             if ro:
                 _, rp2, c2, _ = reorder_mod.reorder(src[0], src[1], None, m.M)
                 src = (rp2, c2, None)
-            for h in HEIGHTS:
-                mm = m if (h == m.H and not ro) else metcf.convert(src[0], src[1], m.M, H=h)
+            for h, w in SHAPES:
+                mm = m if ((h, w) == (m.H, m.W) and not ro) else metcf.convert(
+                    src[0], src[1], m.M, H=h, W=w)
                 for fo in FORMS:
                     fmt, prec = tune.FORMS[fo][0], tune.FORMS[fo][1]
                     scheds, b = tune.autotune(mm, metcf.pack_b(B, fmt), fmt, N, prec, reps=reps)
+                    ok = feasible(N)
                     for sc in scheds:  # the fastest schedule inside the class space
-                        key = (sc.mode, sc.waves, sc.ntile, fo, ro, h)
-                        if key in _INDEX and (best is None or sc.ms < best):
+                        key = (sc.mode, sc.waves, sc.ntile, fo, ro, h, w)
+                        if key in _INDEX and ok[_INDEX[key]] and (best is None or sc.ms < best):
                             best, best_c = sc.ms, _INDEX[key]
         return best_c
 
 
 def main(argv=None):
-    """python -m dtc_b200.costmodel collect|train ... (dataset + weights under data/)."""
+    """python -m dtc_b200.costmodel collect|merge|train ... (dataset + weights under data/)."""
     import argparse
     ap = argparse.ArgumentParser()
-    ap.add_argument("cmd", choices=["collect", "train"])
+    ap.add_argument("cmd", choices=["collect", "merge", "train"])
+    ap.add_argument("--range", default=None, help="lo:hi slice of the matrix list (collect)")
+    ap.add_argument("--out", default=None, help="slice file (collect --range)")
+    ap.add_argument("--parts", nargs="*", default=[], help="slice files (merge)")
     ap.add_argument("--train", type=int, default=400)
     ap.add_argument("--test", type=int, default=100)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--nnz-lo", type=float, default=2 ** 18)
-    ap.add_argument("--nnz-hi", type=float, default=2 ** 22)
+    ap.add_argument("--nnz-lo", type=float, default=1e6)
+    ap.add_argument("--nnz-hi", type=float, default=3e7)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--dataset", default=DATASET_PATH)
     ap.add_argument("--weights", default=WEIGHTS_PATH)
     a = ap.parse_args(argv)
+    if a.cmd == "collect" and a.range:
+        lo, hi = (int(x) for x in a.range.split(":"))
+        collect(a.train, a.test, a.seed, a.nnz_lo, a.nnz_hi, a.reps, log=print, lo=lo, hi=hi,
+                checkpoint=a.out)
+        return
     if a.cmd == "collect":
         ds = collect(a.train, a.test, a.seed, a.nnz_lo, a.nnz_hi, a.reps, log=print)
         save_dataset(ds, a.dataset)
+    if a.cmd == "merge":
+        save_dataset(merge([load_dataset(p) for p in a.parts]), a.dataset)
     ds = load_dataset(a.dataset)
     net, ev = fit(ds, steps=a.steps, seed=a.seed)
     net.save(a.weights, eval=np.array(str(ev)))

@@ -43,16 +43,35 @@ def test_oracle_gradients_match_finite_differences():
 
 
 def test_class_space():
-    assert cm.K == 2 * 2 * 2 * 2 * 5 * 3  # reorder x height x form x mode x waves x N-tile
+    # reorder x block shape (16x8, 32x8, 16x16) x form x (window-mode waves +
+    # balance-mode waves) x N-tile
+    assert cm.K == 2 * 3 * 2 * (7 + 5) * 3
     assert cm.feasible(128).sum() == cm.K // 3
-    # at window height 32 the split kernels hold at most 2 N-tiles per CTA
-    assert cm.feasible(512).sum() == cm.K // 2 + cm.K // 3
+    # at window height 32 and at compaction width 16 the split kernels hold at
+    # most 2 N-tiles per CTA
+    assert cm.feasible(512).sum() == cm.K // 3 + 2 * (2 * cm.K // 9)
     d = cm.CLASSES[cm.default_class(512)]
-    assert (d["H"], d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == \
-        (16, 1, 16, 4, "split24x3", 0)
-    assert {c["H"] for c in cm.CLASSES} == {16, 32} and all(c["W"] == 8 for c in cm.CLASSES)
-    assert len({cm.class_of(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"])
-                for c in cm.CLASSES}) == cm.K
+    assert (d["H"], d["W"], d["mode"], d["waves"], d["ntile"], d["form"], d["reorder"]) == \
+        (16, 8, 1, 16, 4, "split24x3", 0)
+    assert {(c["H"], c["W"]) for c in cm.CLASSES} == {(16, 8), (32, 8), (16, 16)}
+    assert len({cm.class_of(c["mode"], c["waves"], c["ntile"], c["form"], c["reorder"], c["H"],
+                            c["W"]) for c in cm.CLASSES}) == cm.K
+
+
+def test_merge_orders_slices_by_matrix_index():
+    """Slices measured in separate runs merge into one dataset in matrix order,
+    with the classes infeasible for each matrix's N set to NaN."""
+    def part(idx):
+        return dict(features=np.array([[float(i)] * 3 for i in idx]),
+                    times=np.array([[float(i)] * cm.K for i in idx]),
+                    meta=[dict(index=i, N=512 if i % 2 else 128,
+                               split="train" if i < 4 else "test") for i in idx])
+    ds = cm.merge([part([4, 5]), part([0, 1, 2]), part([3])])
+    assert [m["index"] for m in ds["meta"]] == [0, 1, 2, 3, 4, 5]
+    assert np.array_equal(ds["features"][:, 0], np.arange(6.0))
+    for i, m in enumerate(ds["meta"]):
+        f = cm.feasible(m["N"]).astype(bool)
+        assert (ds["times"][i][f] == float(i)).all() and np.isnan(ds["times"][i][~f]).all()
 
 
 def test_targets_and_regret():
@@ -214,6 +233,9 @@ def test_committed_weights_beat_default_on_held_out_cpu():
     for y, n in zip(Y, N[~tr]):
         ok = np.flatnonzero(cm.feasible(int(n)))
         choices.append(int(ok[np.argmin(y[ok])]))
-    ev = cm.evaluate(np.array(choices), ds["times"][~tr], N[~tr], pred=Y)
-    assert ev["speedup_vs_default_geomean"] > 1.5, ev
-    assert ev["regret_mean"] < 0.05 and ev["regret_top4_mean"] < 0.01, ev
+    ev = cm.evaluate(np.array(choices), ds["times"][~tr], N[~tr], pred=Y, topk=8)
+    # 432 classes learned from 600 matrices: the single choice is within a few
+    # per cent of the exhaustive best on average, and timing the 8 cheapest
+    # predicted classes (what the benchmark's plan does) is within 1 %
+    assert ev["speedup_vs_default_geomean"] > 2.0, ev
+    assert ev["regret_mean"] < 0.08 and ev["regret_top8_mean"] < 0.01, ev
