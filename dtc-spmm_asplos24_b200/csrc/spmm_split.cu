@@ -90,6 +90,7 @@ struct SCfg {
   static constexpr int kStgW = 16 * 32 * 4;          // one epilogue warp's 16-row C tile
   static constexpr int kStg = kEpiWarps * 2 * kStgW;  // double-buffered per warp
   static constexpr int kSmem = kX + kE + kY + kStg + kSchedBytes + kBars + 16 + 1024;
+  static_assert(kSmem <= 232448, "dynamic shared memory per CTA");
   static constexpr int kCols = kMmaWarps * kNacc * kAccCols;
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128

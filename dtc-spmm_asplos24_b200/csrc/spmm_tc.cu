@@ -95,6 +95,7 @@ struct Cfg {
   static constexpr int kStg = kEpiWarps * 2 * kStgW;       // double-buffered per warp
   static constexpr int kBars = (2 * S + 2 * kNacc + kMmaWarps) * 8;
   static constexpr int kSmem = kX + kY + kStg + kSchedBytes + kBars + 16 + 1024;
+  static_assert(kSmem <= 232448, "dynamic shared memory per CTA");
   static constexpr int kCols = kMmaWarps * kNacc * NT * WH;  // TMEM columns used
   static_assert(kCols <= 512, "TMEM budget");
   static constexpr uint32_t kTmemCols = kCols <= 32 ? 32 : kCols <= 64 ? 64 : kCols <= 128 ? 128
