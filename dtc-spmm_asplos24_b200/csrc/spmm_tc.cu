@@ -184,6 +184,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_spmm_tf32(const __grid_constant
                          src + (t * 32 + lane) * 4, pad ? 0u : 16u);
           }
         }
+      } else if (nck == 16 || nck == 8) {
+        // 64- or 32-feature rows: 32 / nck gathered rows per warp instruction
+        const int lg = nck == 16 ? 4 : 3;
+        const int sub = lane >> lg, cc = lane & (nck - 1);
+        for (int pb = 0; pb < nb; ++pb) {
+          for (int k0 = 0; k0 < BW; k0 += 32 >> lg) {
+            const int k = k0 + sub;
+            const int32_t r = __shfl_sync(0xffffffffu, rows, pb * BW + k);
+            const bool pad = (k > 0 && r == 0);
+            const float* src = p.B + (int64_t)(pad ? 0 : r) * p.N + col0;
+            cp_async16(xs + (pb * NT * K::kSub + (k >> 3)) * kXTileBytes + x_offset_tf32(k & 7, cc),
+                       src + cc * 4, pad ? 0u : 16u);
+          }
+        }
       } else {
         // partial slice: lanes flattened over (gathered row, 16-byte chunk)
         rows_sm[lw][lane] = rows;

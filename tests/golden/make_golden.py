@@ -32,8 +32,24 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-sys.path.insert(0, os.path.join(ROOT, "oracle", "_ref"))
 import cases  # noqa: E402
+
+
+def _reference_module():
+    """The reference extension built into oracle/_ref, loaded from its file
+    (never through sys.path: importing this module must not shadow the
+    library's own DTCSpMM module of the same name). A process holds one
+    extension module per name, so call this only in a process that does not
+    use the library's DTCSpMM module (this script run on its own)."""
+    import glob
+    import importlib.util
+    found = glob.glob(os.path.join(ROOT, "oracle", "_ref", "DTCSpMM*.so"))
+    if not found:
+        raise RuntimeError("reference extension not built (python oracle/build_ref.py)")
+    spec = importlib.util.spec_from_file_location("DTCSpMM", found[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 @contextlib.contextmanager
@@ -50,7 +66,7 @@ def _in_tmpdir():
 
 def gen_cpu(out):
     import torch
-    import DTCSpMM
+    DTCSpMM = _reference_module()
     for name in cases.CPU_REFERENCE_SAFE:
         rp, col, _, M = cases.CASES[name]()
         nwin = (M + 15) // 16
@@ -94,7 +110,7 @@ def compact(name, arrays):
 
 def gen_gpu(out, shapes, names):
     import torch
-    import DTCSpMM
+    DTCSpMM = _reference_module()
     dev = torch.device("cuda")
     for name in names:
         rp, col, _, M = cases.CASES[name]()
