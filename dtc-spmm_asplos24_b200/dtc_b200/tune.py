@@ -88,7 +88,7 @@ def tune_forms(m: METCF, B: torch.Tensor, max_rel_err=1e-5, reps=3, forms=None):
     """Exhaustive search over (form within the error budget) x schedule.
 
     Returns (best Choice, {form: [measured Schedules]}) -- the table the
-    learned cost model is trained on and judged against.
+    learned cost model is trained on and evaluated against.
     """
     N = B.shape[1]
     forms = forms if forms is not None else eligible_forms(max_rel_err)
