@@ -195,6 +195,37 @@ __global__ void k_score_order(const uint64_t* __restrict__ keys, const int32_t* 
   }
 }
 
+// keys[e] = (cid[r] << 32) | member e of item r's set (one warp per item).
+__global__ void k_cluster_keys(const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                               const int32_t* __restrict__ cid, int32_t n,
+                               uint64_t* __restrict__ keys) {
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = warp; r < n; r += nwarps) {
+    const uint64_t hi = (uint64_t)(uint32_t)cid[r] << 32;
+    for (int64_t e = ptr[r] + lane; e < ptr[r + 1]; e += 32) keys[e] = hi | (uint32_t)idx[e];
+  }
+}
+
+// CSR of the sorted distinct (cluster, member) keys: ptr[c] = first key of
+// cluster c (binary search), idx[i] = member of key i.
+__global__ void k_cluster_csr(const uint64_t* __restrict__ keys, int64_t nk, int32_t nc,
+                              int64_t* __restrict__ ptr, int32_t* __restrict__ idx) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nk; i += stride)
+    idx[i] = (int32_t)(keys[i] & 0xffffffffu);
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= nc; c += stride) {
+    const uint64_t key = (uint64_t)(uint32_t)c << 32;
+    int64_t lo = 0, hi = nk;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    ptr[c] = lo;
+  }
+}
+
 // ord[i] = i.
 __global__ void k_iota(int32_t* __restrict__ ord, int64_t n) {
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -223,9 +254,11 @@ LshLayout lsh_layout(int64_t n_keys, int64_t max_pairs) {
   cub::DeviceRadixSort::SortPairs(nullptr, s1, (uint64_t*)nullptr, (uint64_t*)nullptr,
                                   (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n);
   cub::DeviceScan::ExclusiveSum(nullptr, s2, (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)n + 1);
-  cub::DeviceRadixSort::SortKeys(nullptr, s3, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)mp);
+  // (the raw pairs, and the cluster-member keys of the second level, n of them)
+  const size_t ns = n > mp ? n : mp;
+  cub::DeviceRadixSort::SortKeys(nullptr, s3, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)ns);
   cub::DeviceSelect::Unique(nullptr, s5, (uint64_t*)nullptr, (uint64_t*)nullptr,
-                            (int64_t*)nullptr, (int64_t)mp);
+                            (int64_t*)nullptr, (int64_t)ns);
   cub::DeviceRadixSort::SortPairsDescending(nullptr, s4, (double*)nullptr, (double*)nullptr,
                                             (int32_t*)nullptr, (int32_t*)nullptr, (int64_t)mp);
   L.sort1 = take(s1);
@@ -496,7 +529,7 @@ dtc_status dtc_tca_workspace_bytes(int32_t num_nodes, int64_t nnz, const dtc_tca
   const int64_t nk = n * p.bands;
   DTC_REQUIRE(nk * p.bucket_window < (int64_t)INT32_MAX,
               "num_nodes * bands * bucket_window must fit in int32");
-  const LshLayout L = lsh_layout(nk, nk * p.bucket_window);
+  const LshLayout L = lsh_layout(nk > nnz ? nk : nnz, nk * p.bucket_window);
   size_t off = align_up((size_t)n * p.num_perm * 4, 256) * 2;  // row + cluster signatures
   off += align_up((size_t)n * 4, 256);                          // cluster id per row
   off += align_up((size_t)(n + 1) * 8, 256);                    // item sets: offsets
@@ -579,7 +612,7 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
   };
   const int64_t nk = (int64_t)M * p.bands;
   const int64_t max_pairs = nk * p.bucket_window;
-  const LshLayout L = lsh_layout(nk, max_pairs);
+  const LshLayout L = lsh_layout(nk > nnz ? nk : nnz, max_pairs);
 
   // ---- level 1: rows
   k_row_signatures<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(d_rowptr, d_col, M, p.num_perm,
@@ -593,29 +626,47 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
   const auto groups1 = groups_of(greedy_merge(rows, pairs, M, p.thres));
   const int32_t nc = (int32_t)groups1.size();
 
-  // ---- level 2: clusters, each with the union of its rows' sets
+  // ---- level 2: clusters, each with the union of its rows' sets, built on
+  // the GPU from the rows' sets (still in d_set_ptr / d_set_idx) by sorting
+  // (cluster, member) keys in the banding stage's bytes (dead between levels)
   std::vector<int32_t> hcid(M);
-  Sets cl;
-  cl.ptr.resize(nc + 1);
-  cl.ptr[0] = 0;
-  for (int32_t c = 0; c < nc; ++c) {
-    std::vector<int32_t> u;
-    for (int32_t r : groups1[c]) {
-      hcid[r] = c;
-      u.insert(u.end(), rows.idx.begin() + rows.ptr[r], rows.idx.begin() + rows.ptr[r + 1]);
-    }
-    std::sort(u.begin(), u.end());
-    u.erase(std::unique(u.begin(), u.end()), u.end());
-    cl.idx.insert(cl.idx.end(), u.begin(), u.end());
-    cl.ptr[c + 1] = (int64_t)cl.idx.size();
-  }
+  for (int32_t c = 0; c < nc; ++c)
+    for (int32_t r : groups1[c]) hcid[r] = c;
   DTC_CUDA(cudaMemcpyAsync(cid, hcid.data(), (size_t)M * 4, cudaMemcpyHostToDevice, st));
   DTC_CUDA(cudaMemsetAsync(csig, 0xff, (size_t)nc * p.num_perm * 4, st));
   k_cluster_signatures<<<grid_for((int64_t)M * p.num_perm), kThreads, 0, st>>>(rsig, cid, M,
                                                                               p.num_perm, csig);
   DTC_CUDA(cudaGetLastError());
-  s = upload(cl);
-  if (s != DTC_OK) return s;
+  Sets cl;
+  cl.ptr.assign((size_t)nc + 1, 0);
+  {
+    const int64_t nm = rows.ptr[M];  // members over all rows
+    uint64_t* kin = (uint64_t*)(lws + L.keys_in);
+    uint64_t* kout = (uint64_t*)(lws + L.keys_out);
+    int64_t* nsel = (int64_t*)(lws + L.nsel);
+    int64_t nu = 0;
+    if (nm > 0) {
+      k_cluster_keys<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(d_set_ptr, d_set_idx, cid, M,
+                                                                      kin);
+      DTC_CUDA(cudaGetLastError());
+      size_t b3 = L.uniq - L.sort2;
+      DTC_CUDA(cub::DeviceRadixSort::SortKeys(lws + L.sort2, b3, kin, kout, nm, 0, 64, st));
+      size_t b4 = L.uniq_bytes;
+      DTC_CUDA(cub::DeviceSelect::Unique(lws + L.uniq, b4, kout, kin, nsel, nm, st));
+      DTC_CUDA(cudaMemcpyAsync(&nu, nsel, 8, cudaMemcpyDeviceToHost, st));
+      DTC_CUDA(cudaStreamSynchronize(st));
+    }
+    k_cluster_csr<<<grid_for((nu > nc ? nu : nc) + 1), kThreads, 0, st>>>(kin, nu, nc, d_set_ptr,
+                                                                         d_set_idx);
+    DTC_CUDA(cudaGetLastError());
+    cl.idx.resize((size_t)nu);
+    DTC_CUDA(cudaMemcpyAsync(cl.ptr.data(), d_set_ptr, ((size_t)nc + 1) * 8,
+                             cudaMemcpyDeviceToHost, st));
+    if (nu > 0)
+      DTC_CUDA(cudaMemcpyAsync(cl.idx.data(), d_set_idx, (size_t)nu * 4, cudaMemcpyDeviceToHost,
+                               st));
+    DTC_CUDA(cudaStreamSynchronize(st));
+  }
   s = lsh_pairs(csig, nc, p, lws, L, max_pairs, d_set_ptr, d_set_idx, st, pairs);
   if (s != DTC_OK) return s;
   const auto groups2 = groups_of(greedy_merge(cl, pairs, nc, p.c_thres));
