@@ -312,16 +312,21 @@ def measure(spec, reps=3, device="cuda"):
 
 
 def collect(n_train, n_test, seed=0, nnz_lo=1e6, nnz_hi=3e7, reps=3, log=None, lo=0, hi=None,
-            checkpoint=None):
+            checkpoint=None, n_override=None, index_offset=0):
     """Measured dataset over seeded synthetic matrices (train, then held-out).
 
     The matrix list depends only on the seed and the counts, so [lo, hi) picks
     a slice that can be measured in a separate run and merged later; with
     `checkpoint` the slice measured so far is saved after every matrix. A
     matrix whose measurement fails (a workspace beyond device memory) is
-    logged and left out."""
+    logged and left out. `n_override` fixes every matrix's N (a list drawn from
+    another seed widens the training set to another width); `index_offset`
+    keeps such a list's matrix indices apart from the first one's."""
     rng = np.random.default_rng(seed)
     specs = [sample_spec(rng, nnz_lo, nnz_hi) for _ in range(n_train + n_test)]
+    if n_override:
+        for sp in specs:
+            sp["N"] = int(n_override)
     hi = len(specs) if hi is None else min(hi, len(specs))
     F, Tm, meta = [], [], []
     for i in range(lo, hi):
@@ -336,7 +341,8 @@ def collect(n_train, n_test, seed=0, nnz_lo=1e6, nnz_hi=3e7, reps=3, log=None, l
             continue
         F.append(f)
         Tm.append(t)
-        meta.append(dict(sp, **info, index=i, split="train" if i < n_train else "test"))
+        meta.append(dict(sp, **info, index=i + index_offset,
+                         split="train" if i < n_train else "test"))
         if log:
             log(f"[{i + 1}/{len(specs)}] {sp['family']} N={sp['N']} nnz={info['nnz']} "
                 f"best={np.nanmin(t):.3f}ms {time.perf_counter() - t0:.1f}s")
@@ -508,6 +514,8 @@ def main(argv=None):
     ap.add_argument("--range", default=None, help="lo:hi slice of the matrix list (collect)")
     ap.add_argument("--out", default=None, help="slice file (collect --range)")
     ap.add_argument("--parts", nargs="*", default=[], help="slice files (merge)")
+    ap.add_argument("--N", type=int, default=0, help="fixed N for every matrix (collect)")
+    ap.add_argument("--index-offset", type=int, default=0, help="added to matrix indices")
     ap.add_argument("--train", type=int, default=400)
     ap.add_argument("--test", type=int, default=100)
     ap.add_argument("--seed", type=int, default=0)
@@ -521,7 +529,7 @@ def main(argv=None):
     if a.cmd == "collect" and a.range:
         lo, hi = (int(x) for x in a.range.split(":"))
         collect(a.train, a.test, a.seed, a.nnz_lo, a.nnz_hi, a.reps, log=print, lo=lo, hi=hi,
-                checkpoint=a.out)
+                checkpoint=a.out, n_override=a.N or None, index_offset=a.index_offset)
         return
     if a.cmd == "collect":
         ds = collect(a.train, a.test, a.seed, a.nnz_lo, a.nnz_hi, a.reps, log=print)
