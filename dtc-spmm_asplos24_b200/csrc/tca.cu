@@ -32,7 +32,6 @@
 #include <cub/cub.cuh>
 #include <algorithm>
 #include <queue>
-#include <unordered_set>
 #include <vector>
 #include "common.cuh"
 
@@ -384,6 +383,65 @@ struct Sets {
   }
 };
 
+// Set of pair keys (a << 32 | b, a, b < 2^31): open addressing with linear
+// probing and tombstones, rehashed at half load. Holds the requeued pairs
+// currently in the merge heap.
+class PairSet {
+ public:
+  PairSet() { rehash(1024); }
+  bool contains(uint64_t k) const {
+    for (size_t i = slot(k);; i = (i + 1) & mask_) {
+      if (t_[i] == k) return true;
+      if (t_[i] == kEmpty) return false;
+    }
+  }
+  void insert(uint64_t k) {
+    if (2 * (used_ + 1) > t_.size()) rehash(live_ * 4 > 1024 ? live_ * 4 : 1024);
+    size_t tomb = SIZE_MAX;
+    for (size_t i = slot(k);; i = (i + 1) & mask_) {
+      if (t_[i] == k) return;
+      if (t_[i] == kTomb && tomb == SIZE_MAX) tomb = i;
+      if (t_[i] == kEmpty) {
+        if (tomb != SIZE_MAX) {
+          t_[tomb] = k;
+        } else {
+          t_[i] = k;
+          ++used_;
+        }
+        ++live_;
+        return;
+      }
+    }
+  }
+  void erase(uint64_t k) {
+    for (size_t i = slot(k);; i = (i + 1) & mask_) {
+      if (t_[i] == k) {
+        t_[i] = kTomb;
+        --live_;
+        return;
+      }
+      if (t_[i] == kEmpty) return;
+    }
+  }
+
+ private:
+  static constexpr uint64_t kEmpty = ~0ull, kTomb = ~0ull - 1;
+  std::vector<uint64_t> t_;
+  size_t mask_ = 0, used_ = 0, live_ = 0;  // used_: live + tombstones
+  size_t slot(uint64_t k) const { return (size_t)((k * 0x9E3779B97F4A7C15ull) >> 20) & mask_; }
+  void rehash(size_t want) {
+    size_t cap = 1024;
+    while (cap < 2 * want) cap <<= 1;
+    std::vector<uint64_t> old;
+    old.swap(t_);
+    t_.assign(cap, kEmpty);
+    mask_ = cap - 1;
+    used_ = live_ = 0;
+    for (uint64_t k : old)
+      if (k != kEmpty && k != kTomb) insert(k);
+  }
+};
+
 struct QItem {
   double s;
   int32_t a, b;
@@ -421,14 +479,14 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n,
   for (int32_t a = 0; a < n; ++a) first[a + 1] += first[a];
   int64_t next = 0;  // initial pairs before `next` have been popped
   std::priority_queue<QItem> q;
-  std::unordered_set<uint64_t> requeued;  // pairs currently in the heap
+  PairSet requeued;  // pairs currently in the heap
   // a pair is queued when it is an initial pair not popped yet, or in the heap
   auto queued = [&](uint64_t k) {
     const size_t a = (size_t)(k >> 32);
     const auto b = sp.keys.begin() + first[a], e = sp.keys.begin() + first[a + 1];
     const auto it = std::lower_bound(b, e, k);
     if (it != e && *it == k && rank[it - sp.keys.begin()] >= next) return true;
-    return requeued.count(k) > 0;
+    return requeued.contains(k);
   };
   int64_t num_cluster = n;
   while (num_cluster > 0) {
