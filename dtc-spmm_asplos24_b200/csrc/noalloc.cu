@@ -1,7 +1,7 @@
 // Strict-balance SpMM for callers that cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA-graph
-// capture or a memory-budgeted serving process, plugins whose host forbids
+// Some callers cannot call cudaMalloc: a serving process that has handed all
+// device memory to its own budgeted pool, plugins whose host forbids
 // allocations on the hot path, and plain-C users without an allocator. The
 // regular strict-balance entry point (dtc_spmm_balance) needs a caller-sized
 // workspace for its window-offset table and per-CTA partial tiles; this

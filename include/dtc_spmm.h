@@ -212,7 +212,7 @@ dtc_status dtc_spmm_balance(const int32_t* d_tcblockRowid, const uint8_t* d_tile
 
 /* Strict-balance SpMM that allocates nothing and takes no workspace; no
  * counterpart in the reference. For callers that cannot call cudaMalloc
- * (inside a CUDA-graph capture, in a memory-budgeted server, in plugins or
+ * (a server whose device memory belongs to its own budgeted pool, plugins or
  * plain-C hosts without a device allocator): the window-offset table and the
  * partial tiles live in a fixed 16 MiB array compiled into the library, held
  * in the memory of every GPU that loads it until the process exits.

@@ -1,6 +1,6 @@
 """GPU test of dtc_spmm_balance_noalloc, the strict-balance SpMM for callers that
-cannot allocate device memory (graph captures, memory-budgeted servers,
-plugins without an allocator): it keeps its scratch in an array compiled into
+cannot allocate device memory (servers whose device memory belongs to their
+own budgeted pool, plugins without an allocator): it keeps its scratch in an array compiled into
 the library instead of a caller workspace.
 
 Called through the C ABI and compared, within the TF32 tolerance of
