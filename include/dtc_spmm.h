@@ -280,7 +280,9 @@ typedef struct {
 } dtc_schedule;
 
 /* Fills out[0..min(count, max_out)) with every schedule the kernels support for
- * N and returns the count (out may be NULL to query it). */
+ * N and returns the count (out may be NULL to query it): waves 1, 2, 4, 8, 16,
+ * 32 and 64 in window mode, 1 to 16 in balance mode (whose cut windows keep
+ * partial tiles per chunk), times the N-tiles the kernels hold for N. */
 int dtc_schedule_candidates(int32_t N, dtc_schedule* out, int max_out);
 /* The same for a given window height and kernel family (split = 1 for the
  * split-precision forms, whose N-tiles per CTA are capped at 2 at height 32). */
@@ -292,7 +294,8 @@ dtc_status dtc_autotune_workspace_bytes(int32_t num_nodes, int64_t num_blocks, i
                                         int32_t block_h, size_t* bytes);
 
 /* Times every candidate (one untimed run + `reps` runs between CUDA events on
- * `stream`; synchronises it) on the given ME-TCF arrays and B form, writes the
+ * `stream`; synchronises it; split forms at block width 16 skip N-tile counts
+ * above 2, which those kernels cap) on the given ME-TCF arrays and B form, writes the
  * measured schedules to results[0..max_results), their count to *num_results
  * and the index of the fastest to *best. d_C receives the last candidate's
  * product. Arguments as in dtc_spmm_ex. */
