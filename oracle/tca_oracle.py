@@ -20,8 +20,13 @@ dtc_tca_reorder, so that the library's permutation can be checked bit-exactly:
   their clusters ascending, each cluster's rows ascending.
 
 The reference's own MinHash and LSH come from datasketch / libMHCUDA and its
-Jaccard from cuGraph, none of which are installed; the permutation is
-therefore not comparable to the reference's, only to this restatement.
+Jaccard from cuGraph, none of which are installed, so the library's LSH
+candidates are not comparable to the reference's. Everything after the
+candidates (two_level: the merge, level 2 and the output order) is pinned to
+the reference script itself: tests/golden/ref_tca_*.npz hold its reorder_id
+for candidates given by threshold_pairs (tests/golden/make_tca_golden.py).
+The one open detail, the order of equal similarities (the script's Pair
+compares similarity only), is (p1, p2) ascending here and in those fixtures.
 """
 import heapq
 
@@ -155,6 +160,37 @@ def groups_of(roots):
     return groups
 
 
+def two_level(rows, pairs1, pairs2_of, thres, c_thres):
+    """The two clustering levels and the output order (TCA_reorder.py:154-307).
+
+    rows: the rows' column sets; pairs1: level-1 candidate pairs (lo, hi);
+    pairs2_of(g1, csets): level-2 candidate pairs over the level-1 clusters g1
+    (in order of first appearance) whose column sets are csets (the union of
+    their rows' sets). The candidate rule is the caller's: the library's LSH
+    (tca_perm) or any other rule fed to the reference's own merge."""
+    g1 = groups_of(greedy_merge(rows, pairs1, thres))
+    csets = [np.unique(np.concatenate([np.asarray(rows[i], np.int64) for i in g])) for g in g1]
+    g2 = groups_of(greedy_merge(csets, pairs2_of(g1, csets), c_thres))
+    return np.array([row for g in g2 for c in g for row in g1[c]], np.int32)
+
+
+def threshold_pairs(sets, thr):
+    """Pairs (lo, hi) of nonempty sets whose exact Jaccard is >= thr: an
+    exact stand-in for MinHash LSH at threshold thr."""
+    n = len(sets)
+    ss = [set(int(x) for x in s) for s in sets]
+    out = []
+    for a in range(n):
+        if not ss[a]:
+            continue
+        for b in range(a + 1, n):
+            if ss[b]:
+                inter = len(ss[a] & ss[b])
+                if inter / len(ss[a] | ss[b]) >= thr:
+                    out.append((a, b))
+    return out
+
+
 def tca_perm(rowptr, col, M, **params):
     p = dict(DEFAULTS, **params)
     rowptr = np.asarray(rowptr, np.int64)
@@ -162,8 +198,8 @@ def tca_perm(rowptr, col, M, **params):
     rows = [np.unique(col[rowptr[i]:rowptr[i + 1]]) for i in range(M)]
     P, b, r, w = p["num_perm"], p["bands"], p["rows_per_band"], p["bucket_window"]
     rsig = signatures(rows, P, p["seed"])
-    g1 = groups_of(greedy_merge(rows, lsh_pairs(rsig, b, r, w), p["thres"]))
-    csets = [np.unique(np.concatenate([rows[i] for i in g])) for g in g1]
-    csig = np.stack([rsig[g].min(axis=0) for g in g1]).astype(np.uint32)
-    g2 = groups_of(greedy_merge(csets, lsh_pairs(csig, b, r, w), p["c_thres"]))
-    return np.array([row for g in g2 for c in g for row in g1[c]], np.int32)
+
+    def pairs2_of(g1, csets):
+        csig = np.stack([rsig[g].min(axis=0) for g in g1]).astype(np.uint32)
+        return lsh_pairs(csig, b, r, w)
+    return two_level(rows, lsh_pairs(rsig, b, r, w), pairs2_of, p["thres"], p["c_thres"])

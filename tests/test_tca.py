@@ -1,7 +1,13 @@
 """TCA reorder (reordering/TCA_reorder.py:53-326): the library's permutation is
 bit-exact with the oracle's restatement (same hashing, banding and merge
 rules), is a permutation, respects the level-1 cluster cap, and reduces the
-ME-TCF block count on a matrix with hidden row clusters."""
+ME-TCF block count on a matrix with hidden row clusters. The oracle's merge,
+level-2 clustering and output order are pinned to the reference script's own
+run (tests/golden/ref_tca_*.npz, made by tests/golden/make_tca_golden.py with
+exact-threshold candidates in place of MinHash LSH)."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
@@ -33,6 +39,35 @@ def test_oracle_clusters_respect_caps():
     sizes = np.bincount(roots)
     # a cluster stops growing once it reaches the cap; the last merge can overshoot
     assert sizes.max() < 2 * 16
+
+
+TCA_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_tca_*.npz")))
+LSH_THRES = 0.2      # lsh_thres and cluster_thres of the script (TCA_reorder.py:21-23)
+C_THRES = 128        # c_thres (TCA_reorder.py:22)
+
+
+def test_tca_golden_present():
+    assert len(TCA_GOLDEN) >= 6
+
+
+@pytest.mark.parametrize("path", TCA_GOLDEN, ids=lambda p: os.path.basename(p)[8:-4])
+def test_oracle_merge_matches_reference_script(path):
+    """Same candidate pairs (exact Jaccard >= 0.2 at both levels, the rule the
+    script's MinHash LSH approximates) -> the reference's reorder_id, bit for
+    bit: merge order and direction, the cluster cap, requeues of roots with
+    their own sets, level-2 clustering at cap 128 and the output order."""
+    z = np.load(path)
+    n, src, dst = int(z["num_nodes"]), z["src_li"], z["dst_li"]
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    rp = np.searchsorted(src, np.arange(n + 1)).astype(np.int64)
+    rows = [np.unique(dst[rp[i]:rp[i + 1]]) for i in range(n)]
+    assert all(len(r) for r in rows)
+    assert int(z["ties"][0]) > 0  # the tie rule is exercised
+    perm = TO.two_level(rows, TO.threshold_pairs(rows, LSH_THRES),
+                        lambda g1, csets: TO.threshold_pairs(csets, LSH_THRES),
+                        int(z["thres"]), C_THRES)
+    np.testing.assert_array_equal(perm, z["reorder_id"])
 
 
 def test_oracle_mix64_matches_vectorised():
