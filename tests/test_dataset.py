@@ -1,8 +1,16 @@
 """Graph .npz loader (scripts/DTCSpMM/dataset.py:21-44): src_li / dst_li /
 num_nodes -> CSR with every edge = 1 and duplicates summed, bit-exact with
-scipy's coo -> csr (the reference's call) and the oracle."""
+scipy's coo -> csr (the reference's call), the oracle, and the reference
+loader's own output (tests/golden/ref_loader_*.npz, made by
+tests/golden/make_loader_golden.py)."""
+import glob
+import os
+
 import numpy as np
 import pytest
+
+LOADER_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden",
+                                              "ref_loader_*.npz")))
 
 from oracle import oracle as O
 
@@ -25,6 +33,32 @@ def test_oracle_coo_rebuild_matches_scipy():
     np.testing.assert_array_equal(rp, S.indptr)
     np.testing.assert_array_equal(c, S.indices)
     np.testing.assert_array_equal(v, S.data.astype(np.float32))
+
+
+def test_loader_golden_present():
+    assert len(LOADER_GOLDEN) >= 3
+
+
+@pytest.mark.parametrize("path", LOADER_GOLDEN, ids=lambda p: os.path.basename(p)[11:-4])
+def test_oracle_matches_reference_loader(path):
+    z = np.load(path)
+    n = int(z["num_nodes"])
+    rp, c, v = O._coo_to_csr(z["src_li"], z["dst_li"], None, n, n)
+    np.testing.assert_array_equal(rp, z["row_pointers"])
+    np.testing.assert_array_equal(c, z["column_index"])
+    assert rp[-1] == rp[-2]  # the last node has no edges
+    assert (v > 1).any()     # duplicate edges were summed
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", LOADER_GOLDEN, ids=lambda p: os.path.basename(p)[11:-4])
+def test_load_npz_matches_reference_loader(cuda, path):
+    from dtc_b200 import dataset
+    rp, col, val, n = dataset.load_npz(path)
+    z = np.load(path)
+    assert n == int(z["num_nodes"])
+    np.testing.assert_array_equal(rp.cpu().numpy(), z["row_pointers"])
+    np.testing.assert_array_equal(col.cpu().numpy(), z["column_index"])
 
 
 @pytest.mark.gpu
