@@ -20,6 +20,10 @@ reference's own code:
 * The dataset load and the two result files go to memory (np.load / np.savez
   are redirected for the script's run); nothing is written anywhere else.
 
+Each fixture also holds the reference pipeline's reordered CSR: the script's
+relabelled edge list (its second result file) read by the reference's own
+graph loader (scripts/DTCSpMM/dataset.py, see make_loader_golden.py).
+
 The one detail the script leaves open is the order of equal similarities:
 its Pair.__lt__ compares similarity alone, so Python's heap pops tied pairs
 in an order fixed by the heap's history (and, through the insertion order, by
@@ -45,9 +49,12 @@ import os
 import queue
 import runpy
 import sys
+import tempfile
 import types
 
 import numpy as np
+
+import make_loader_golden  # this folder: the reference graph loader
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_ROOT = os.environ.get("DTC_REFERENCE_ROOT", "/root/reference")
@@ -226,6 +233,7 @@ def run_reference(src, dst, n, thres, name="case"):
                 sys.modules[k] = v
     reorder = np.asarray(store[name + ".reorder_id.npz"]["reorder_id"], np.int32)
     stats = [(q.pops, q.ties) for q in TieOrderedQueue.made]
+    run_reference.relabelled = store[name + ".reorder.npz"]
     return reorder, stats
 
 
@@ -237,8 +245,19 @@ def main():
         reorder, stats = run_reference(src, dst, n, thres, name)
         assert len(stats) == 2, stats
         print(f"{name}: pops {[p for p, _ in stats]}, pops that met a tie {[t for _, t in stats]}")
+        # the reference pipeline's reordered CSR: the script's relabelled edge
+        # list (TCA_reorder.py:316-326) read back by its graph loader
+        rel = run_reference.relabelled
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, name + ".reorder.npz")
+            np.savez(path, src_li=np.asarray(rel["src_li"], np.int64),
+                     dst_li=np.asarray(rel["dst_li"], np.int64), num_nodes=np.int64(n))
+            g = make_loader_golden._reference_loader()(path)
+            rrp = g.row_pointers.numpy().astype(np.int32)
+            rcol = g.column_index.numpy().astype(np.int32)
         np.savez_compressed(os.path.join(HERE, f"ref_tca_{name}.npz"), src_li=src, dst_li=dst,
                             num_nodes=np.int64(n), thres=np.int64(thres), reorder_id=reorder,
+                            reordered_row_pointers=rrp, reordered_column_index=rcol,
                             pops=np.array([p for p, _ in stats], np.int64),
                             ties=np.array([t for _, t in stats], np.int64))
 

@@ -11,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from oracle import tca_oracle as TO
 
 
@@ -68,6 +69,38 @@ def test_oracle_merge_matches_reference_script(path):
                         lambda g1, csets: TO.threshold_pairs(csets, LSH_THRES),
                         int(z["thres"]), C_THRES)
     np.testing.assert_array_equal(perm, z["reorder_id"])
+
+
+def _golden_csr(z):
+    n, src, dst = int(z["num_nodes"]), z["src_li"], z["dst_li"]
+    order = np.lexsort((dst, src))
+    src, dst = src[order], dst[order]
+    return np.searchsorted(src, np.arange(n + 1)).astype(np.int32), dst.astype(np.int32), n
+
+
+@pytest.mark.parametrize("path", TCA_GOLDEN, ids=lambda p: os.path.basename(p)[8:-4])
+def test_oracle_relabel_matches_reference_pipeline(path):
+    """P A P^T with the script's reorder_id equals the reference pipeline's
+    reordered CSR: its relabelled edge list (TCA_reorder.py:316-326) read by
+    its graph loader (scripts/DTCSpMM/dataset.py:21-44)."""
+    z = np.load(path)
+    rp, col, n = _golden_csr(z)
+    orp, oc, _ = O.permute_csr(rp, col, None, z["reorder_id"].astype(np.int64))
+    np.testing.assert_array_equal(orp, z["reordered_row_pointers"])
+    np.testing.assert_array_equal(oc, z["reordered_column_index"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", TCA_GOLDEN, ids=lambda p: os.path.basename(p)[8:-4])
+def test_permute_matches_reference_pipeline(cuda, path):
+    import torch
+    from dtc_b200 import metcf
+    z = np.load(path)
+    rp, col, n = _golden_csr(z)
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    grp, gc, _ = metcf.permute_csr(g(rp), g(col), None, g(z["reorder_id"].astype(np.int32)))
+    np.testing.assert_array_equal(grp.cpu().numpy(), z["reordered_row_pointers"])
+    np.testing.assert_array_equal(gc.cpu().numpy(), z["reordered_column_index"])
 
 
 def test_oracle_mix64_matches_vectorised():
