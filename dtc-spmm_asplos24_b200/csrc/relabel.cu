@@ -43,23 +43,33 @@ __global__ void k_invert(const int32_t* __restrict__ perm, int32_t M, int32_t* _
 }
 
 // Checks the input CSR (rowptr[0] == 0, non-decreasing, rowptr[M] == nnz,
-// 0 <= col < K) and writes the old row of every edge.
+// 0 <= col < K) and writes the old row of every edge. Edge-parallel: thread e
+// finds its row by binary search, the last r in [0, M) with rowptr[r] <= e
+// (for a valid CSR the row holding e; empty rows before it share its start and
+// lose to it). Neighbouring edges take the same search path, so a warp's loads
+// are mostly broadcasts of cached entries, and a hub row of tens of thousands
+// of entries costs no more than as many short rows (with a warp per row, one
+// warp would walk each hub row alone). Every probe reads rowptr[1 .. M-1], so
+// an invalid CSR stays in bounds; it sets the error bit and is rejected by the
+// host before erow is read.
 __global__ void k_rows(const int32_t* __restrict__ rowptr, const int32_t* __restrict__ col,
                        int32_t M, int32_t K, int64_t nnz, int32_t* __restrict__ erow,
                        uint32_t* bad) {
-  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = warp; r < M; r += nwarps) {
-    const int32_t e0 = rowptr[r], e1 = rowptr[r + 1];
-    if (lane == 0 && (e1 < e0 || (r == 0 && e0 != 0) || (r == M - 1 && e1 != nnz)))
-      atomicOr(bad, 2u);
-    if (e0 < 0 || e1 > nnz || e1 < e0) continue;
-    for (int32_t e = e0 + lane; e < e1; e += 32) {
-      erow[e] = (int32_t)r;
-      const int32_t c = col[e];
-      if (c < 0 || c >= K) atomicOr(bad, 2u);
+  const int64_t t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = t0; r < M; r += stride) {
+    const int32_t e0 = __ldg(rowptr + r), e1 = __ldg(rowptr + r + 1);
+    if (e1 < e0 || (r == 0 && e0 != 0) || (r == M - 1 && e1 != nnz)) atomicOr(bad, 2u);
+  }
+  for (int64_t e = t0; e < nnz; e += stride) {
+    int32_t lo = 0, hi = M;  // rowptr[lo] <= e (rowptr[0] == 0), and hi == M or rowptr[hi] > e
+    while (hi - lo > 1) {
+      const int32_t mid = lo + ((hi - lo) >> 1);
+      if (__ldg(rowptr + mid) <= e) lo = mid; else hi = mid;
     }
+    erow[e] = lo;
+    const int32_t c = __ldg(col + e);
+    if (c < 0 || c >= K) atomicOr(bad, 2u);
   }
 }
 
@@ -208,7 +218,8 @@ dtc_status relabel(int mode, const int32_t* rowptr, const int32_t* col, const fl
   if (mode == 2) {
     if (nnz > 0) k_coo_rows<<<grid_for(nnz), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow, bad);
   } else if (M > 0) {
-    k_rows<<<grid_for((int64_t)M * 32), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow, bad);
+    k_rows<<<grid_for(nnz > M ? nnz : (int64_t)M), kThreads, 0, st>>>(rowptr, col, M, K, nnz, erow,
+                                                                     bad);
   }
   uint32_t hbad = 0;
   DTC_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st));

@@ -61,6 +61,8 @@ def main(argv=None):
     val = torch.from_numpy(A.val).to(dev)
     if a.kernel in ("tca", "permute", "transpose", "coo"):
         return _relabel(a, dev, A, name, rp, col, val)
+    if a.kernel == "features":  # the schedule features are defined on the 16 x 8 ME-TCF
+        a.H, a.W = 16, 8
     m = metcf.convert(rp, col, A.M, H=a.H, W=a.W, values=val, device=dev)
     B = torch.from_numpy(gen.normal(A.K, a.N, seed=1)).to(dev)
     fmt, prec = tune.FORMS[a.form][0], tune.FORMS[a.form][1]
