@@ -31,6 +31,7 @@
 // Items with an empty set never enter LSH and stay singletons.
 #include <cub/cub.cuh>
 #include <algorithm>
+#include <new>
 #include <queue>
 #include <vector>
 #include "common.cuh"
@@ -740,3 +741,67 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
 }
 
 }  // extern "C"
+
+namespace {
+
+// The body of dtc_tca_merge (host memory throughout; no CUDA call).
+dtc_status merge_host(const int64_t* set_ptr, const int32_t* set_idx, int32_t n,
+                      const uint64_t* pairs, int64_t num_pairs, int32_t cap, int32_t* roots) {
+  DTC_REQUIRE(n >= 0 && num_pairs >= 0, "negative sizes");
+  DTC_REQUIRE(num_pairs < (int64_t)INT32_MAX, "num_pairs must fit in int32");
+  DTC_REQUIRE(cap >= 1, "cap must be at least 1");
+  DTC_REQUIRE(n == 0 || (set_ptr && roots), "null host pointer");
+  DTC_REQUIRE(num_pairs == 0 || pairs, "null host pointer");
+  if (n == 0) return DTC_OK;
+  Sets sets;
+  sets.ptr.assign(set_ptr, set_ptr + (size_t)n + 1);
+  DTC_REQUIRE(sets.ptr[0] == 0, "set_ptr[0] must be 0");
+  for (int32_t i = 0; i < n; ++i)
+    DTC_REQUIRE(sets.ptr[i + 1] >= sets.ptr[i], "set_ptr must be non-decreasing");
+  const int64_t total = sets.ptr[n];
+  DTC_REQUIRE(total == 0 || set_idx, "null host pointer");
+  sets.idx.assign(set_idx, set_idx + total);
+  for (int32_t i = 0; i < n; ++i)
+    for (int64_t e = sets.ptr[i] + 1; e < sets.ptr[i + 1]; ++e)
+      DTC_REQUIRE(sets.idx[e - 1] < sets.idx[e], "every set must be sorted and distinct");
+  // the hand-over of lsh_pairs: distinct keys ascending, then the score order
+  // (descending Jaccard, ties in ascending pair order) and each key's rank in it
+  Scored sp;
+  sp.keys.assign(pairs, pairs + num_pairs);
+  for (uint64_t k : sp.keys)
+    DTC_REQUIRE((k >> 32) < (k & 0xffffffffu) && (k & 0xffffffffu) < (uint64_t)n,
+                "pairs must be lo << 32 | hi with lo < hi < num_items");
+  std::sort(sp.keys.begin(), sp.keys.end());
+  sp.keys.erase(std::unique(sp.keys.begin(), sp.keys.end()), sp.keys.end());
+  const int64_t np = (int64_t)sp.keys.size();
+  std::vector<double> s((size_t)np);
+  for (int64_t j = 0; j < np; ++j)
+    s[j] = sets.jac((int32_t)(sp.keys[j] >> 32), (int32_t)(sp.keys[j] & 0xffffffffu));
+  std::vector<int64_t> order((size_t)np);
+  for (int64_t j = 0; j < np; ++j) order[j] = j;
+  std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return s[x] > s[y]; });
+  sp.skey.resize(np);
+  sp.score.resize(np);
+  sp.rank.resize(np);
+  for (int64_t r = 0; r < np; ++r) {
+    sp.skey[r] = sp.keys[order[r]];
+    sp.score[r] = s[order[r]];
+    sp.rank[order[r]] = (int32_t)r;
+  }
+  const std::vector<int32_t> r = greedy_merge(sets, sp, n, cap);
+  std::copy(r.begin(), r.end(), roots);
+  return DTC_OK;
+}
+
+}  // namespace
+
+extern "C" dtc_status dtc_tca_merge(const int64_t* set_ptr, const int32_t* set_idx,
+                                    int32_t num_items, const uint64_t* pairs, int64_t num_pairs,
+                                    int32_t cap, int32_t* roots) {
+  try {
+    return merge_host(set_ptr, set_idx, num_items, pairs, num_pairs, cap, roots);
+  } catch (const std::bad_alloc&) {
+    set_error("dtc_tca_merge: out of host memory");
+    return DTC_ERR_INVALID_ARGUMENT;
+  }
+}

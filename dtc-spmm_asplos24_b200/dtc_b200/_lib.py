@@ -57,6 +57,7 @@ SIGNATURES = {
     "dtc_mlp_argmin": [vp, vp, C.c_int, i32, i32, vp, vp],
     "dtc_tca_workspace_bytes": [i32, i64, vp, szp],
     "dtc_tca_reorder": [vp, vp, i32, i64, vp, vp, vp, sz, vp],
+    "dtc_tca_merge": [vp, vp, i32, vp, i64, i32, vp],
     "dtc_permute_csr": [vp, vp, vp, i32, i64, vp, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_transpose_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],
     "dtc_coo_to_csr": [vp, vp, vp, i32, i32, i64, vp, vp, vp, i64p, vp, sz, vp],

@@ -3,6 +3,7 @@ application (dtc_permute_csr), the GPU form of reordering/TCA_reorder.py and
 the CSR rebuild of scripts/DTCSpMM/dataset.py:38-44."""
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -37,3 +38,23 @@ def reorder(rowptr, col, val, num_nodes, params=None):
     perm = tca_perm(rowptr, col, num_nodes, params)
     rp, c, v = permute_csr(rowptr, col, val, perm)
     return perm, rp, c, v
+
+
+def merge_pairs(sets, pairs, cap):
+    """One level of the TCA greedy merge on given candidate pairs (dtc_tca_merge,
+    host memory, no GPU): ``sets`` are the items' column sets (sequences of
+    ints), ``pairs`` (lo, hi) candidate pairs; returns the root of every item
+    (int32 numpy array)."""
+    n = len(sets)
+    norm = [np.unique(np.asarray(x, np.int64)) for x in sets]
+    ptr = np.zeros(n + 1, np.int64)
+    if n:
+        ptr[1:] = np.cumsum([len(x) for x in norm])
+    idx = (np.concatenate(norm) if n and ptr[-1] else np.zeros(1, np.int64)).astype(np.int32)
+    pr = np.asarray(pairs, np.uint64).reshape(-1, 2)
+    keys = np.ascontiguousarray((pr[:, 0] << np.uint64(32)) | pr[:, 1]) if len(pr) else \
+        np.zeros(1, np.uint64)
+    roots = np.zeros(max(n, 1), np.int32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    call("dtc_tca_merge", p(ptr), p(idx), n, p(keys), len(pr), int(cap), p(roots))
+    return roots[:n]

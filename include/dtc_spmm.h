@@ -143,6 +143,25 @@ dtc_status dtc_tca_reorder(const int32_t* d_rowptr, const int32_t* d_col, int32_
                            int64_t nnz, const dtc_tca_params* params, int32_t* d_perm,
                            void* d_workspace, size_t workspace_bytes, dtc_stream_t stream);
 
+/* One level of the TCA greedy merge on caller-given candidate pairs, in HOST
+ * memory (no CUDA call): the merge loop of reordering/TCA_reorder.py:153-188
+ * (level 1, cap `thres`) and :252-294 (level 2, cap `c_thres`), which
+ * dtc_tca_reorder runs on its own LSH candidates. No counterpart entry in the
+ * reference (its merge runs inline in the script); it lets a caller with
+ * another candidate generator (for example datasketch's MinHash LSH) reuse the
+ * merge. Items are num_items sets, CSR of sorted distinct members
+ * (set_ptr[num_items+1], set_idx[set_ptr[num_items]]); pairs[num_pairs] are
+ * lo << 32 | hi with lo < hi (duplicates ignored). Pairs pop by descending
+ * Jaccard, equal scores in ascending (first, second) order; two roots merge,
+ * the smaller cluster into the larger and equal sizes into the first member; a
+ * cluster reaching `cap` is closed; a pair whose ends are not both roots is
+ * requeued once as (root of first, root of second), keeping that orientation,
+ * with the Jaccard of the two root items' own sets. Writes the
+ * root of every item to roots[num_items]. Level 2 runs it again on the level-1
+ * clusters (sets = the union of their rows' sets). */
+dtc_status dtc_tca_merge(const int64_t* set_ptr, const int32_t* set_idx, int32_t num_items,
+                         const uint64_t* pairs, int64_t num_pairs, int32_t cap, int32_t* roots);
+
 /* COO edge list -> canonical CSR: the CSR build of the reference's loader
  * (scripts/DTCSpMM/dataset.py:21-44: src_li / dst_li / num_nodes of an .npz,
  * coo_matrix((1, (src, dst))).tocsr()). d_val == NULL gives every edge the

@@ -103,6 +103,55 @@ def test_permute_matches_reference_pipeline(cuda, path):
     np.testing.assert_array_equal(gc.cpu().numpy(), z["reordered_column_index"])
 
 
+def _two_level_with(merge, rows, thres):
+    """Level 1 and level 2 with `merge(sets, pairs, cap) -> roots` on
+    exact-threshold candidates, composed in the order of TCA_reorder.py:300-307."""
+    g1 = TO.groups_of(merge(rows, TO.threshold_pairs(rows, LSH_THRES), thres))
+    csets = [np.unique(np.concatenate([rows[i] for i in g])) for g in g1]
+    g2 = TO.groups_of(merge(csets, TO.threshold_pairs(csets, LSH_THRES), C_THRES))
+    return np.array([row for g in g2 for c in g for row in g1[c]], np.int32)
+
+
+@pytest.mark.parametrize("path", TCA_GOLDEN, ids=lambda p: os.path.basename(p)[8:-4])
+def test_library_merge_matches_reference_script(path):
+    """The library's own merge loop (dtc_tca_merge: the greedy_merge that
+    dtc_tca_reorder runs, host code, no GPU) at both levels reproduces the
+    reference script's reorder_id from the same candidates."""
+    from dtc_b200 import reorder
+    z = np.load(path)
+    rp, col, n = _golden_csr(z)
+    rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(n)]
+    got = _two_level_with(lambda sets, pairs, cap: reorder.merge_pairs(sets, pairs, cap),
+                          rows, int(z["thres"]))
+    np.testing.assert_array_equal(got, z["reorder_id"])
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_library_merge_matches_oracle_on_lsh_pairs(seed):
+    """Same roots as the oracle's greedy_merge on the library's LSH candidate
+    rule (many equal scores, requeues, both caps)."""
+    from dtc_b200 import reorder
+    rp, col, M = clustered(M=300, groups=20, seed=seed)
+    rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(M)]
+    pairs = TO.lsh_pairs(TO.signatures(rows, 128, 2022), 42, 3, 8)
+    for cap in (2, 4, 16):
+        np.testing.assert_array_equal(reorder.merge_pairs(rows, pairs, cap),
+                                      TO.greedy_merge(rows, pairs, cap))
+
+
+def test_library_merge_rejects_bad_input():
+    from dtc_b200 import _lib, reorder
+    rows = [np.array([0, 1]), np.array([1, 2]), np.array([5])]
+    with pytest.raises(_lib.DtcError):
+        reorder.merge_pairs(rows, [(1, 0)], 4)          # lo > hi
+    with pytest.raises(_lib.DtcError):
+        reorder.merge_pairs(rows, [(0, 3)], 4)          # hi out of range
+    with pytest.raises(_lib.DtcError):
+        reorder.merge_pairs(rows, [(0, 1)], 0)          # cap < 1
+    assert reorder.merge_pairs([], [], 4).shape == (0,)
+    np.testing.assert_array_equal(reorder.merge_pairs(rows, [], 4), [0, 1, 2])
+
+
 def test_oracle_mix64_matches_vectorised():
     xs = [0, 1, 2 ** 63 + 5, 123456789]
     np.testing.assert_array_equal(TO._mix64_np(np.array(xs, np.uint64)),
