@@ -58,3 +58,28 @@ def merge_pairs(sets, pairs, cap):
     p = lambda a: a.ctypes.data_as(C.c_void_p)
     call("dtc_tca_merge", p(ptr), p(idx), n, p(keys), len(pr), int(cap), p(roots))
     return roots[:n]
+
+
+def cluster_order(sets, candidates, thres=16, c_thres=128):
+    """The two-level TCA clustering on a caller's candidate rule, host only:
+    ``candidates(sets) -> [(lo, hi), ...]`` is called on the rows' column
+    sets, then on the level-1 clusters' sets (the union of their rows' sets);
+    each level merges with dtc_tca_merge (caps ``thres`` rows and ``c_thres``
+    clusters). Returns perm[new] = old in the reference's output order
+    (reordering/TCA_reorder.py:190-200, :296-307): level-2 groups by first
+    appearance, their clusters ascending, each cluster's rows ascending. With
+    the library's LSH as the rule this is what dtc_tca_reorder computes."""
+    rows = [np.unique(np.asarray(x, np.int64)) for x in sets]
+
+    def groups(roots):
+        gid, out = {}, []
+        for i, r in enumerate(roots.tolist()):
+            if r not in gid:
+                gid[r] = len(out)
+                out.append([])
+            out[gid[r]].append(i)
+        return out
+    g1 = groups(merge_pairs(rows, candidates(rows), thres))
+    csets = [np.unique(np.concatenate([rows[i] for i in g])) for g in g1]
+    g2 = groups(merge_pairs(csets, candidates(csets), c_thres))
+    return np.array([r for g in g2 for c in g for r in g1[c]], np.int32)

@@ -103,26 +103,17 @@ def test_permute_matches_reference_pipeline(cuda, path):
     np.testing.assert_array_equal(gc.cpu().numpy(), z["reordered_column_index"])
 
 
-def _two_level_with(merge, rows, thres):
-    """Level 1 and level 2 with `merge(sets, pairs, cap) -> roots` on
-    exact-threshold candidates, composed in the order of TCA_reorder.py:300-307."""
-    g1 = TO.groups_of(merge(rows, TO.threshold_pairs(rows, LSH_THRES), thres))
-    csets = [np.unique(np.concatenate([rows[i] for i in g])) for g in g1]
-    g2 = TO.groups_of(merge(csets, TO.threshold_pairs(csets, LSH_THRES), C_THRES))
-    return np.array([row for g in g2 for c in g for row in g1[c]], np.int32)
-
-
 @pytest.mark.parametrize("path", TCA_GOLDEN, ids=lambda p: os.path.basename(p)[8:-4])
 def test_library_merge_matches_reference_script(path):
-    """The library's own merge loop (dtc_tca_merge: the greedy_merge that
-    dtc_tca_reorder runs, host code, no GPU) at both levels reproduces the
-    reference script's reorder_id from the same candidates."""
+    """The library's host clustering (reorder.cluster_order: both levels on
+    dtc_tca_merge, the greedy_merge that dtc_tca_reorder runs; no GPU)
+    reproduces the reference script's reorder_id from the same candidates."""
     from dtc_b200 import reorder
     z = np.load(path)
     rp, col, n = _golden_csr(z)
     rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(n)]
-    got = _two_level_with(lambda sets, pairs, cap: reorder.merge_pairs(sets, pairs, cap),
-                          rows, int(z["thres"]))
+    got = reorder.cluster_order(rows, lambda sets: TO.threshold_pairs(sets, LSH_THRES),
+                                int(z["thres"]), C_THRES)
     np.testing.assert_array_equal(got, z["reorder_id"])
 
 
@@ -137,6 +128,19 @@ def test_library_merge_matches_oracle_on_lsh_pairs(seed):
     for cap in (2, 4, 16):
         np.testing.assert_array_equal(reorder.merge_pairs(rows, pairs, cap),
                                       TO.greedy_merge(rows, pairs, cap))
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_cluster_order_with_lsh_rule_is_tca_perm(seed):
+    """cluster_order on the library's LSH candidate rule is the oracle's
+    tca_perm (which dtc_tca_reorder equals bit for bit on the GPU): at level 2
+    the signature of a cluster's union is the min of its rows' signatures."""
+    from dtc_b200 import reorder
+    rp, col, M = clustered(M=320, groups=24, seed=seed)
+    rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(M)]
+    rule = lambda sets: TO.lsh_pairs(TO.signatures(sets, 128, 2022), 42, 3, 8)
+    np.testing.assert_array_equal(reorder.cluster_order(rows, rule, 8, 16),
+                                  TO.tca_perm(rp, col, M, thres=8, c_thres=16))
 
 
 def test_library_merge_rejects_bad_input():
