@@ -54,6 +54,9 @@ def test_bad_arguments_return_status_not_exit():
     assert L.dtc_spmm(None, None, None, None, None, 16, 1, 1, None, 16, None, None) == 1
     assert L.dtc_spmm_ex(None, None, None, None, None, 16, 1, 1, 16, 8, 0, None, None, 16, 0,
                          None, 7, 0, 0, None, 0, None) == 1
+    assert L.dtc_tca_merge(None, None, 3, None, 0, 4, None) == 1  # host entry: null sets
+    assert b"null" in L.dtc_last_error()
+    assert L.dtc_tca_merge(None, None, 0, None, 0, 4, None) == 0  # no items: nothing to do
 
 
 def test_bformat_sizes():
