@@ -365,11 +365,32 @@ dtc_status lsh_pairs(const uint32_t* sig, int32_t n, const dtc_tca_params& prm, 
 // Jaccard |a ∩ b| / |a ∪ b| of two sorted, distinct lists (0 when either is empty).
 double jaccard(const int32_t* a, int64_t na, const int32_t* b, int64_t nb) {
   if (na == 0 || nb == 0) return 0.0;
-  int64_t i = 0, j = 0, inter = 0;
-  while (i < na && j < nb) {
-    if (a[i] < b[j]) ++i;
-    else if (a[i] > b[j]) ++j;
-    else { ++inter; ++i; ++j; }
+  if (na > nb) {  // a is the smaller list
+    std::swap(a, b);
+    std::swap(na, nb);
+  }
+  int64_t inter = 0;
+  if (na * 32 < nb) {
+    // sizes far apart (a hub row against a short one): gallop through b for
+    // each member of a, O(na log nb) instead of O(na + nb)
+    int64_t j = 0;
+    for (int64_t i = 0; i < na && j < nb; ++i) {
+      const int32_t x = a[i];
+      int64_t step = 1, hi = j;
+      while (hi < nb && b[hi] < x) { j = hi + 1; hi += step; step <<= 1; }
+      if (hi > nb) hi = nb;
+      j = std::lower_bound(b + j, b + hi, x) - b;
+      if (j < nb && b[j] == x) { ++inter; ++j; }
+    }
+  } else {
+    // branchless merge: each step advances past the smaller head (both on a match)
+    int64_t i = 0, j = 0;
+    while (i < na && j < nb) {
+      const int32_t x = a[i], y = b[j];
+      inter += (x == y);
+      i += (x <= y);
+      j += (y <= x);
+    }
   }
   return (double)inter / (double)(na + nb - inter);
 }
@@ -458,16 +479,22 @@ struct QItem {
 // root) pairs go to a heap, and the next pair is the better of the two heads
 // in the QItem order.
 std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n, int32_t cap) {
-  std::vector<int32_t> parent(n), size(n, 1);
-  std::vector<char> deleted(n, 0);
-  for (int32_t i = 0; i < n; ++i) parent[i] = i;
+  // Per item, packed so that one cache line serves each item the loop touches:
+  // the union-find parent and the cluster size, negated once the cluster is
+  // closed (the size of a closed cluster is never read again).
+  struct Node {
+    int32_t parent, size;
+  };
+  std::vector<Node> node((size_t)n);
+  for (int32_t i = 0; i < n; ++i) node[i] = {i, 1};
   auto root = [&](int32_t i) {
-    while (i != parent[i]) {
-      parent[i] = parent[parent[i]];
-      i = parent[i];
+    while (i != node[i].parent) {
+      node[i].parent = node[node[i].parent].parent;
+      i = node[i].parent;
     }
     return i;
   };
+  auto closed = [&](int32_t i) { return node[i].size < 0; };
   auto key = [](int32_t a, int32_t b) {
     return a < b ? ((uint64_t)a << 32) | (uint32_t)b : ((uint64_t)b << 32) | (uint32_t)a;
   };
@@ -489,6 +516,9 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n,
     if (it != e && *it == k && rank[it - sp.keys.begin()] >= next) return true;
     return requeued.contains(k);
   };
+  // the initial pairs are walked in a known order: fetch the nodes of the pair
+  // kAhead places further while this one is handled
+  constexpr int64_t kAhead = 16;
   int64_t num_cluster = n;
   while (num_cluster > 0) {
     QItem it;
@@ -505,29 +535,39 @@ std::vector<int32_t> greedy_merge(const Sets& sets, const Scored& sp, int32_t n,
       break;
     }
     if (from_init) {
+      if (next + kAhead < np) {
+        const uint64_t kf = sp.skey[next + kAhead];
+        __builtin_prefetch(&node[kf >> 32]);
+        __builtin_prefetch(&node[kf & 0xffffffffu]);
+        // second stage: the parents of the pair kAhead / 2 places on (their
+        // nodes were fetched kAhead / 2 pops ago), the first step of root()
+        const uint64_t kh = sp.skey[next + kAhead / 2];
+        __builtin_prefetch(&node[node[kh >> 32].parent]);
+        __builtin_prefetch(&node[node[kh & 0xffffffffu].parent]);
+      }
       ++next;
     } else {
       q.pop();
       requeued.erase(key(it.a, it.b));
     }
     int32_t p1 = it.a, p2 = it.b;
-    if (p1 == parent[p1] && p2 == parent[p2]) {
-      if (deleted[p1] || deleted[p2]) continue;
-      if (size[p1] < size[p2]) {
-        parent[p1] = p2;
-        --num_cluster;
-        size[p2] += size[p1];
-        if (size[p2] >= cap) { deleted[p2] = 1; --num_cluster; }
+    if (p1 == node[p1].parent && p2 == node[p2].parent) {
+      if (closed(p1) || closed(p2)) continue;
+      const int32_t s1 = node[p1].size, s2 = node[p2].size;
+      --num_cluster;
+      if (s1 < s2) {
+        node[p1].parent = p2;
+        node[p2].size = s1 + s2;
+        if (s1 + s2 >= cap) { node[p2].size = -(s1 + s2); --num_cluster; }
       } else {
-        parent[p2] = p1;
-        --num_cluster;
-        size[p1] += size[p2];
-        if (size[p1] >= cap) { deleted[p1] = 1; --num_cluster; }
+        node[p2].parent = p1;
+        node[p1].size = s1 + s2;
+        if (s1 + s2 >= cap) { node[p1].size = -(s1 + s2); --num_cluster; }
       }
     } else {
       p1 = root(p1);
       p2 = root(p2);
-      if (deleted[p1] || deleted[p2]) continue;
+      if (closed(p1) || closed(p2)) continue;
       if (p1 != p2 && !queued(key(p1, p2))) {
         q.push({sets.jac(p1, p2), p1, p2});
         requeued.insert(key(p1, p2));
