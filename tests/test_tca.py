@@ -143,6 +143,23 @@ def test_cluster_order_with_lsh_rule_is_tca_perm(seed):
                                   TO.tca_perm(rp, col, M, thres=8, c_thres=16))
 
 
+@pytest.mark.parametrize("seed", range(6))
+def test_library_merge_matches_oracle_fuzz(seed):
+    """Random small sets (some empty, many overlapping) and random candidate
+    pairs: equal and zero scores everywhere, requeues and caps from 1 to 8;
+    the library's roots equal the oracle's."""
+    from dtc_b200 import reorder
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(2, 80))
+    sets = [np.unique(rng.integers(0, 12, int(rng.integers(0, 6)))) for _ in range(n)]
+    m = int(rng.integers(0, 4 * n))
+    pairs = sorted({(int(min(a, b)), int(max(a, b)))
+                    for a, b in rng.integers(0, n, (m, 2)) if a != b})
+    for cap in (1, 2, 3, 8):
+        np.testing.assert_array_equal(reorder.merge_pairs(sets, pairs, cap),
+                                      TO.greedy_merge(sets, pairs, cap))
+
+
 def test_library_merge_rejects_bad_input():
     from dtc_b200 import _lib, reorder
     rows = [np.array([0, 1]), np.array([1, 2]), np.array([5])]
