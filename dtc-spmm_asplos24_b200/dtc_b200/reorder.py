@@ -42,15 +42,24 @@ def reorder(rowptr, col, val, num_nodes, params=None):
 
 def merge_pairs(sets, pairs, cap):
     """One level of the TCA greedy merge on given candidate pairs (dtc_tca_merge,
-    host memory, no GPU): ``sets`` are the items' column sets (sequences of
-    ints), ``pairs`` (lo, hi) candidate pairs; returns the root of every item
-    (int32 numpy array)."""
-    n = len(sets)
-    norm = [np.unique(np.asarray(x, np.int64)) for x in sets]
-    ptr = np.zeros(n + 1, np.int64)
-    if n:
-        ptr[1:] = np.cumsum([len(x) for x in norm])
-    idx = (np.concatenate(norm) if n and ptr[-1] else np.zeros(1, np.int64)).astype(np.int32)
+    host memory, no GPU): ``sets`` are the items' column sets, either a
+    sequence of integer sequences or a tuple ``(ptr, idx)`` of CSR arrays
+    whose rows are already sorted and distinct (the library checks); ``pairs``
+    are (lo, hi) candidate pairs. Returns the root of every item (int32 numpy
+    array)."""
+    if isinstance(sets, tuple):
+        ptr = np.ascontiguousarray(sets[0], np.int64)
+        idx = np.ascontiguousarray(sets[1], np.int32)
+        n = len(ptr) - 1
+        if idx.size == 0:
+            idx = np.zeros(1, np.int32)
+    else:
+        n = len(sets)
+        norm = [np.unique(np.asarray(x, np.int64)) for x in sets]
+        ptr = np.zeros(n + 1, np.int64)
+        if n:
+            ptr[1:] = np.cumsum([len(x) for x in norm])
+        idx = (np.concatenate(norm) if n and ptr[-1] else np.zeros(1, np.int64)).astype(np.int32)
     pr = np.asarray(pairs, np.uint64).reshape(-1, 2)
     keys = np.ascontiguousarray((pr[:, 0] << np.uint64(32)) | pr[:, 1]) if len(pr) else \
         np.zeros(1, np.uint64)

@@ -160,6 +160,19 @@ def test_library_merge_matches_oracle_fuzz(seed):
                                       TO.greedy_merge(sets, pairs, cap))
 
 
+def test_library_merge_accepts_csr_sets():
+    from dtc_b200 import _lib, reorder
+    rp, col, M = clustered(M=200, groups=12, seed=5)
+    rows = [np.unique(col[rp[i]:rp[i + 1]]) for i in range(M)]
+    ptr = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
+    idx = np.concatenate(rows)
+    pairs = TO.lsh_pairs(TO.signatures(rows, 128, 2022), 42, 3, 8)
+    np.testing.assert_array_equal(reorder.merge_pairs((ptr, idx), pairs, 8),
+                                  reorder.merge_pairs(rows, pairs, 8))
+    with pytest.raises(_lib.DtcError):  # rows must be sorted and distinct
+        reorder.merge_pairs((np.array([0, 2]), np.array([3, 1])), [], 4)
+
+
 def test_library_merge_rejects_bad_input():
     from dtc_b200 import _lib, reorder
     rows = [np.array([0, 1]), np.array([1, 2]), np.array([5])]
